@@ -1,0 +1,1032 @@
+// Host side of the C ABI (include/atum_b200.h): operator and solver objects,
+// brick geometry, kernel dispatch and the time-stepping drivers.
+//
+// There is no CPU compute path: every operator application, stage update,
+// banded solve and reduction runs on the GPU; the host only sequences launches
+// (and, for the relaxation RK, runs the scalar trust-region Newton on device
+// reductions).
+#include "../../include/atum_b200.h"
+#include "atb_generic.cuh"
+#include "atb_reduce.cuh"
+#include "atb_tendency.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace atb;
+
+namespace atb {
+template <> tend_launch_fn pick_launcher<LAW_ADV>(int, int);
+template <> tend_launch_fn pick_launcher<LAW_EULER>(int, int);
+template <> tend_launch_fn pick_launcher<LAW_EG>(int, int);
+template <> tend_launch_fn pick_launcher<LAW_LEG>(int, int);
+template <> tend_launch_fn pick_launcher<LAW_SW>(int, int);
+template <> red_launch_fn pick_reducer<LAW_ADV>(int);
+template <> red_launch_fn pick_reducer<LAW_EULER>(int);
+template <> red_launch_fn pick_reducer<LAW_EG>(int);
+template <> red_launch_fn pick_reducer<LAW_LEG>(int);
+template <> red_launch_fn pick_reducer<LAW_SW>(int);
+}  // namespace atb
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CK(call)                                                                                   \
+  do {                                                                                             \
+    cudaError_t _e = (call);                                                                       \
+    if (_e != cudaSuccess) return fail(ATB_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(_e));    \
+  } while (0)
+
+int check_launch(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(ATB_ERR_CUDA, "%s launch: %s", what, cudaGetErrorString(e));
+  return ATB_OK;
+}
+
+template <class T> int dalloc(T** p, size_t n) {
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return fail(ATB_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+  }
+  return ATB_OK;
+}
+
+// ------------------------------------------------------------ profiling
+constexpr int NPROF = 5;
+struct Prof {
+  bool on = false;
+  long launches_total = 0;
+  long n[NPROF] = {0, 0, 0, 0, 0};
+  double ms[NPROF] = {0, 0, 0, 0, 0};
+  std::vector<cudaEvent_t> pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+  cudaEvent_t get() {
+    if (!pool.empty()) {
+      cudaEvent_t e = pool.back();
+      pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+  void resolve() {
+    for (auto& p : pending) {
+      cudaEventSynchronize(p.second.second);
+      float t = 0;
+      cudaEventElapsedTime(&t, p.second.first, p.second.second);
+      ms[p.first] += t;
+      n[p.first] += 1;
+      pool.push_back(p.second.first);
+      pool.push_back(p.second.second);
+    }
+    pending.clear();
+  }
+};
+Prof g_prof;
+
+// brackets one launch: construct before, call done() after
+struct ProfScope {
+  int k;
+  cudaStream_t st;
+  cudaEvent_t a = nullptr;
+  ProfScope(int kclass, cudaStream_t s) : k(kclass), st(s) {
+    g_prof.launches_total++;
+    if (g_prof.on) {
+      a = g_prof.get();
+      cudaEventRecord(a, st);
+    }
+  }
+  ~ProfScope() {
+    if (a) {
+      cudaEvent_t b = g_prof.get();
+      cudaEventRecord(b, st);
+      g_prof.pending.push_back({k, {a, b}});
+    }
+  }
+};
+
+}  // namespace
+
+struct atb_op {
+  LawP law{};
+  int dim = 0, N = 0, Nq = 0, Np = 0, Nfp = 0, K = 0, Kd[3] = {1, 1, 1}, ns = 0, naux = 0;
+  int vk = 0, dirs = 0, sflux = 0, precision = 0, stacked = 0;
+  int naux_used = 0;  // leading aux components the tendency kernel stages
+  std::vector<double> w, D;
+  double* d_ginv = nullptr;
+  int* d_nbr = nullptr;
+  double* d_aux = nullptr;
+  double* d_tab = nullptr;
+  double* d_w = nullptr;
+  double* d_J = nullptr;
+  double* d_partials = nullptr;
+  double* d_red = nullptr;
+  double* h_red = nullptr;
+  int red_blocks = 0;
+  tend_launch_fn launch = nullptr;
+  red_launch_fn reducer = nullptr;
+  int prof_class = ATB_PROF_TEND;
+  int E = 1;
+  size_t smem = 0;
+  size_t stride() const { return (size_t)K * Np; }
+  int elem_of(const int* idx) const {
+    if (stacked) {
+      int ev = idx[dim - 1], eh = 0, m = 1;
+      for (int d = 0; d < dim - 1; ++d) { eh += idx[d] * m; m *= Kd[d]; }
+      return eh * Kd[dim - 1] + ev;
+    }
+    int e = 0, m = 1;
+    for (int d = 0; d < dim; ++d) { e += idx[d] * m; m *= Kd[d]; }
+    return e;
+  }
+};
+
+namespace {
+
+void fill_args(const atb_op* op, TendArgs& A) {
+  A.K = op->K;
+  A.Nq = op->Nq;
+  A.Np = op->Np;
+  A.Nfp = op->Nfp;
+  A.E = op->E;
+  A.naux = op->naux_used;
+  A.ginv = op->d_ginv;
+  A.nbr = op->d_nbr;
+  A.aux = op->d_aux;
+  A.tab = op->d_tab;
+  A.law = op->law;
+  A.dirs = op->dirs;
+  A.sflux = op->sflux;
+  A.stride = op->stride();
+  A.a = 0;
+  A.bdt = 0;
+}
+
+// one tendency launch: epi with input q, outputs out/out2
+int run_tendency(atb_op* op, int epi, const double* const* q, double* const* out, double* const* out2, double a,
+                 double bdt, cudaStream_t st) {
+  TendArgs A;
+  fill_args(op, A);
+  A.epi = epi;
+  A.a = a;
+  A.bdt = bdt;
+  for (int s = 0; s < 5; ++s) {
+    A.q[s] = q[s < op->ns ? s : 0];
+    A.out[s] = out ? out[s < op->ns ? s : 0] : nullptr;
+    A.out2[s] = out2 ? out2[s < op->ns ? s : 0] : nullptr;
+  }
+  int grid = (op->K + op->E - 1) / op->E;
+  {
+    ProfScope ps(op->prof_class, st);
+    op->launch(A, grid, op->E * op->Np, op->smem, st);
+  }
+  return check_launch("tendency");
+}
+
+void field_ptrs(double* base, int ns, size_t stride, double** p) {
+  for (int s = 0; s < 5; ++s) p[s] = base + (size_t)(s < ns ? s : 0) * stride;
+}
+
+int reduce(atb_op* op, int kind, const double* const* p, const double* const* q, double* out5, cudaStream_t st) {
+  RedArgs R;
+  R.K = op->K;
+  R.Nq = op->Nq;
+  R.Np = op->Np;
+  R.naux = op->naux;
+  R.kind = kind;
+  R.w = op->d_w;
+  R.J = op->d_J;
+  R.aux = op->d_aux;
+  R.law = op->law;
+  R.stride = op->stride();
+  for (int s = 0; s < 5; ++s) {
+    R.p[s] = p[s < op->ns ? s : 0];
+    R.q[s] = q ? q[s < op->ns ? s : 0] : R.p[s];
+  }
+  R.partials = op->d_partials;
+  {
+    ProfScope ps(ATB_PROF_REDUCE, st);
+    op->reducer(R, op->red_blocks, st);
+  }
+  int rc = check_launch("reduce");
+  if (rc) return rc;
+  {
+    ProfScope ps(ATB_PROF_REDUCE, st);
+    launch_red_finish(op->d_partials, op->red_blocks, kind == RED_LINF, op->d_red, st);
+  }
+  rc = check_launch("reduce finish");
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(op->h_red, op->d_red, 5 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  for (int k = 0; k < 5; ++k) out5[k] = op->h_red[k];
+  return ATB_OK;
+}
+
+}  // namespace
+
+// =================================================================== op
+extern "C" int atb_version(void) { return 1; }
+extern "C" const char* atb_last_error(void) { return g_err.c_str(); }
+extern "C" int atb_device_count(int* n) {
+  CK(cudaGetDeviceCount(n));
+  return ATB_OK;
+}
+
+extern "C" int atb_op_destroy(atb_op* op) {
+  if (!op) return ATB_OK;
+  cudaFree(op->d_ginv);
+  cudaFree(op->d_nbr);
+  cudaFree(op->d_aux);
+  cudaFree(op->d_tab);
+  cudaFree(op->d_w);
+  cudaFree(op->d_J);
+  cudaFree(op->d_partials);
+  cudaFree(op->d_red);
+  if (op->h_red) cudaFreeHost(op->h_red);
+  delete op;
+  return ATB_OK;
+}
+
+extern "C" int atb_op_create(const atb_op_desc* d, const double* aux_host, atb_op** out) {
+  if (!d || !out) return fail(ATB_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (d->dim < 1 || d->dim > 3) return fail(ATB_ERR_INVALID, "dim must be 1..3");
+  if (d->N < 1 || d->N > 7) return fail(ATB_ERR_INVALID, "polynomial order N must be 1..7");
+  if (d->law < 0 || d->law > 4) return fail(ATB_ERR_INVALID, "unknown law %d", d->law);
+  if (d->precision != ATB_PREC_FP64) return fail(ATB_ERR_INVALID, "precision %d is not built", d->precision);
+  if (!d->lgl_weights || !d->lgl_D) return fail(ATB_ERR_INVALID, "LGL tables missing");
+  if (d->naux < 0 || d->naux > 8) return fail(ATB_ERR_INVALID, "naux must be 0..8");
+  if (d->naux > 0 && !aux_host) return fail(ATB_ERR_INVALID, "aux fields missing");
+  if ((d->directions & ((1 << d->dim) - 1)) == 0 || (d->directions >> d->dim))
+    return fail(ATB_ERR_INVALID, "directions must be a non-empty subset of 1:dim");
+  int vk = VK_WEAK;
+  if (d->volume_form == 1) {
+    switch (d->volume_flux) {
+      case ATB_FLUX_CENTRAL: vk = VK_CENTRAL; break;
+      case ATB_FLUX_EC: vk = VK_EC; break;
+      case ATB_FLUX_KG: vk = VK_KG; break;
+      default: return fail(ATB_ERR_INVALID, "no two-point volume flux %d", d->volume_flux);
+    }
+  }
+  tend_launch_fn fn = nullptr;
+  red_launch_fn rf = nullptr;
+  switch (d->law) {
+    case LAW_ADV: fn = pick_launcher<LAW_ADV>(d->dim, vk); rf = pick_reducer<LAW_ADV>(d->dim); break;
+    case LAW_EULER: fn = pick_launcher<LAW_EULER>(d->dim, vk); rf = pick_reducer<LAW_EULER>(d->dim); break;
+    case LAW_EG: fn = pick_launcher<LAW_EG>(d->dim, vk); rf = pick_reducer<LAW_EG>(d->dim); break;
+    case LAW_LEG: fn = pick_launcher<LAW_LEG>(d->dim, vk); rf = pick_reducer<LAW_LEG>(d->dim); break;
+    case LAW_SW: fn = pick_launcher<LAW_SW>(d->dim, vk); rf = pick_reducer<LAW_SW>(d->dim); break;
+  }
+  if (!fn) return fail(ATB_ERR_INVALID, "unsupported (law %d, volume flux %d) combination", d->law, d->volume_flux);
+  const int sf = d->surface_flux;
+  bool sf_ok = sf == ATB_FLUX_CENTRAL || sf == ATB_FLUX_RUSANOV;
+  if (d->law == LAW_EULER || d->law == LAW_EG) sf_ok = sf_ok || (sf >= ATB_FLUX_EC && sf <= ATB_FLUX_MATRIX);
+  if (d->law == LAW_SW) sf_ok = sf_ok || sf == ATB_FLUX_EC || sf == ATB_FLUX_ROE;
+  if (!sf_ok) return fail(ATB_ERR_INVALID, "no surface flux %d for law %d", sf, d->law);
+  if (d->law == LAW_SW && d->sw_topography && d->naux < 1 + d->dim)
+    return fail(ATB_ERR_INVALID, "shallow-water topography needs aux = [b, grad b]");
+  if ((d->law == LAW_EG || d->law == LAW_LEG) && d->naux < 1 + d->dim)
+    return fail(ATB_ERR_INVALID, "Euler-gravity laws need aux = [Phi, grad Phi, ...]");
+  if ((d->law == LAW_LEG || (d->law == LAW_EG && d->pde_level_balance)) && d->naux < 3 + d->dim)
+    return fail(ATB_ERR_INVALID, "this law needs the reference state in aux");
+
+  atb_op* op = new atb_op();
+  op->launch = fn;
+  op->reducer = rf;
+  op->dim = d->dim;
+  op->N = d->N;
+  op->Nq = d->N + 1;
+  op->Np = 1;
+  for (int k = 0; k < d->dim; ++k) op->Np *= op->Nq;
+  op->Nfp = op->Np / op->Nq;
+  op->K = 1;
+  for (int k = 0; k < 3; ++k) {
+    op->Kd[k] = k < d->dim ? d->K[k] : 1;
+    if (op->Kd[k] < 1) {
+      delete op;
+      return fail(ATB_ERR_INVALID, "K[%d] must be >= 1", k);
+    }
+    op->K *= op->Kd[k];
+  }
+  op->ns = (d->law == LAW_ADV) ? 1 : d->dim + 2;
+  op->naux = d->naux;
+  op->vk = vk;
+  op->dirs = d->directions;
+  op->sflux = sf;
+  op->precision = d->precision;
+  op->stacked = d->stacked;
+  LawP& L = op->law;
+  L.kind = d->law;
+  L.dim = d->dim;
+  L.ns = op->ns;
+  L.naux = d->naux;
+  L.gamma = d->gamma;
+  L.grav = d->grav;
+  for (int k = 0; k < 3; ++k) { L.adv_u[k] = d->adv_u[k]; L.omega[k] = d->omega[k]; }
+  std::memcpy(L.bc_state, d->bc_state, sizeof(L.bc_state));
+  L.pde = d->pde_level_balance;
+  L.bc = d->bc_kind;
+  L.src = d->source_kind;
+  L.swtopo = d->sw_topography;
+
+  const int Nq = op->Nq, Np = op->Np, K = op->K, dim = op->dim;
+  op->w.assign(d->lgl_weights, d->lgl_weights + Nq);
+  op->D.assign(d->lgl_D, d->lgl_D + Nq * Nq);
+  // tables: Cfd[i][m] = D[m][i] w_m / w_i - D[i][m] (0 on the diagonal),
+  //         Cw[i][m]  = D[m][i] w_m / w_i, lift_end = 1 / w_0
+  std::vector<double> tab(2 * Nq * Nq + 2, 0.0);
+  for (int i = 0; i < Nq; ++i)
+    for (int m = 0; m < Nq; ++m) {
+      double cw = op->D[m * Nq + i] * op->w[m] / op->w[i];
+      tab[i * Nq + m] = (i == m) ? 0.0 : cw - op->D[i * Nq + m];
+      tab[Nq * Nq + i * Nq + m] = cw;
+    }
+  tab[2 * Nq * Nq] = 1.0 / op->w[0];
+  // geometry
+  std::vector<double> ginv((size_t)K * 3, 0.0), J(K, 1.0);
+  std::vector<int> nbr((size_t)K * 6, 0);
+  int idx[3];
+  for (idx[2] = 0; idx[2] < op->Kd[2]; ++idx[2])
+    for (idx[1] = 0; idx[1] < op->Kd[1]; ++idx[1])
+      for (idx[0] = 0; idx[0] < op->Kd[0]; ++idx[0]) {
+        const int e = op->elem_of(idx);
+        double Je = 1.0;
+        for (int k = 0; k < dim; ++k) {
+          const double h = d->vertices[k][idx[k] + 1] - d->vertices[k][idx[k]];
+          if (!(h > 0)) {
+            delete op;
+            return fail(ATB_ERR_INVALID, "vertex vector %d is not increasing", k);
+          }
+          ginv[e * 3 + k] = 2.0 / h;
+          Je *= h / 2;
+        }
+        J[e] = Je;
+        for (int k = 0; k < 3; ++k)
+          for (int f = 0; f < 2; ++f) {
+            int face = 2 * k + f;
+            if (k >= dim) { nbr[e * 6 + face] = -(face + 1); continue; }
+            int nb[3] = {idx[0], idx[1], idx[2]};
+            nb[k] += f ? 1 : -1;
+            if (nb[k] < 0 || nb[k] >= op->Kd[k]) {
+              if (d->periodic[k]) {
+                nb[k] = (nb[k] + op->Kd[k]) % op->Kd[k];
+              } else {
+                nbr[e * 6 + face] = -(face + 1);  // boundary tag = face number
+                continue;
+              }
+            }
+            nbr[e * 6 + face] = op->elem_of(nb);
+          }
+      }
+  // launch shape: E elements per CTA, ~256 threads (>= 1 element)
+  // aux components the kernels read: Euler-gravity needs Phi (fluxes, wave
+  // speeds), grad Phi for the weak form's non-conservative term, and the
+  // reference state under pde_level_balance; the linear law needs all of
+  // them; shallow-water bathymetry needs b (and grad b in the weak form)
+  int nu = 0;
+  if (d->law == LAW_EG) nu = d->pde_level_balance ? dim + 3 : (vk == VK_WEAK ? dim + 1 : 1);
+  if (d->law == LAW_LEG) nu = dim + 3;
+  if (d->law == LAW_SW && d->sw_topography) nu = (vk == VK_WEAK) ? dim + 1 : 1;
+  op->naux_used = std::min(nu, op->naux);
+  const int npre = npre_of(d->law, dim, vk), npv = npv_of(d->law, dim, vk);
+  op->E = std::max(1, 256 / Np);
+  while (op->E > 1 &&
+         tend_smem_bytes(op->ns, npre, op->naux_used, dim, Nq, Np, op->Nfp, op->E, npv) > 100 * 1024)
+    --op->E;
+  op->smem = tend_smem_bytes(op->ns, npre, op->naux_used, dim, Nq, Np, op->Nfp, op->E, npv);
+  if (op->smem > 227 * 1024) {
+    delete op;
+    return fail(ATB_ERR_INVALID, "element too large for shared memory (%zu bytes)", op->smem);
+  }
+  op->red_blocks = 148 * 4;
+  int rc;
+  if ((rc = dalloc(&op->d_ginv, ginv.size())) || (rc = dalloc(&op->d_nbr, nbr.size())) ||
+      (rc = dalloc(&op->d_tab, tab.size())) || (rc = dalloc(&op->d_w, (size_t)Nq)) || (rc = dalloc(&op->d_J, (size_t)K)) ||
+      (rc = dalloc(&op->d_aux, (size_t)std::max(1, op->naux) * K * Np)) ||
+      (rc = dalloc(&op->d_partials, (size_t)op->red_blocks * 5)) || (rc = dalloc(&op->d_red, 5))) {
+    atb_op_destroy(op);
+    return rc;
+  }
+  if (cudaMallocHost((void**)&op->h_red, 5 * sizeof(double)) != cudaSuccess) {
+    op->h_red = nullptr;
+    atb_op_destroy(op);
+    return fail(ATB_ERR_NOMEM, "cudaMallocHost failed");
+  }
+  cudaError_t e1 = cudaMemcpy(op->d_ginv, ginv.data(), ginv.size() * sizeof(double), cudaMemcpyHostToDevice);
+  cudaError_t e2 = cudaMemcpy(op->d_nbr, nbr.data(), nbr.size() * sizeof(int), cudaMemcpyHostToDevice);
+  cudaError_t e3 = cudaMemcpy(op->d_tab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice);
+  cudaError_t e4 = cudaMemcpy(op->d_w, op->w.data(), Nq * sizeof(double), cudaMemcpyHostToDevice);
+  cudaError_t e5 = cudaMemcpy(op->d_J, J.data(), K * sizeof(double), cudaMemcpyHostToDevice);
+  cudaError_t e6 = cudaSuccess;
+  if (op->naux) e6 = cudaMemcpy(op->d_aux, aux_host, (size_t)op->naux * K * Np * sizeof(double), cudaMemcpyHostToDevice);
+  if (e1 || e2 || e3 || e4 || e5 || e6) {
+    atb_op_destroy(op);
+    return fail(ATB_ERR_CUDA, "uploading operator tables failed");
+  }
+  *out = op;
+  return ATB_OK;
+}
+
+extern "C" int atb_op_dims(const atb_op* op, int* ns, int* K, int* Np) {
+  if (!op) return fail(ATB_ERR_INVALID, "null op");
+  if (ns) *ns = op->ns;
+  if (K) *K = op->K;
+  if (Np) *Np = op->Np;
+  return ATB_OK;
+}
+
+extern "C" int atb_op_apply(atb_op* op, double* const* dq, const double* const* q, double time, int increment,
+                            void* stream) {
+  (void)time;  // no time-dependent boundary or source kinds
+  if (!op || !dq || !q) return fail(ATB_ERR_INVALID, "null argument");
+  return run_tendency(op, increment ? EPI_ADD : EPI_SET, q, dq, nullptr, 0, 0, (cudaStream_t)stream);
+}
+
+extern "C" int atb_weightednorm(atb_op* op, const double* const* q, double p, double* comp, double* total,
+                                void* stream) {
+  if (!op || !q) return fail(ATB_ERR_INVALID, "null argument");
+  const bool inf = std::isinf(p);
+  if (!inf && p != 2) return fail(ATB_ERR_INVALID, "weightednorm supports p = 2 and p = Inf");
+  double r[5];
+  int rc = reduce(op, inf ? RED_LINF : RED_L2, q, nullptr, r, (cudaStream_t)stream);
+  if (rc) return rc;
+  double tot = 0, m = 0;
+  for (int s = 0; s < op->ns; ++s) {
+    double v = inf ? r[s] : std::sqrt(r[s]);
+    if (comp) comp[s] = v;
+    tot += v * v;
+    m = std::max(m, v);
+  }
+  if (total) *total = inf ? m : std::sqrt(tot);
+  return ATB_OK;
+}
+
+extern "C" int atb_entropyintegral(atb_op* op, const double* const* q, double* out, void* stream) {
+  if (!op || !q || !out) return fail(ATB_ERR_INVALID, "null argument");
+  double r[5];
+  int rc = reduce(op, RED_ENTROPY, q, nullptr, r, (cudaStream_t)stream);
+  *out = r[0];
+  return rc;
+}
+
+extern "C" int atb_entropyproduct(atb_op* op, const double* const* p, const double* const* q, double* out,
+                                  void* stream) {
+  if (!op || !p || !q || !out) return fail(ATB_ERR_INVALID, "null argument");
+  double r[5];
+  int rc = reduce(op, RED_ENTPROD, p, q, r, (cudaStream_t)stream);
+  *out = r[0];
+  return rc;
+}
+
+extern "C" int atb_check_finite(atb_op* op, const double* const* q, void* stream) {
+  if (!op || !q) return fail(ATB_ERR_INVALID, "null argument");
+  double r[5];
+  int rc = reduce(op, RED_NONFINITE, q, nullptr, r, (cudaStream_t)stream);
+  if (rc) return rc;
+  if (r[0] != 0) return fail(ATB_ERR_NONFINITE, "%g non-finite values in state", r[0]);
+  return ATB_OK;
+}
+
+extern "C" int atb_profile_enable(int on) {
+  g_prof.on = on != 0;
+  return ATB_OK;
+}
+extern "C" int atb_profile_reset(void) {
+  g_prof.resolve();
+  for (int k = 0; k < NPROF; ++k) { g_prof.n[k] = 0; g_prof.ms[k] = 0; }
+  return ATB_OK;
+}
+extern "C" int atb_profile_read(int kclass, long* launches, double* total_ms) {
+  if (kclass < 0 || kclass >= NPROF) return fail(ATB_ERR_INVALID, "profile class %d", kclass);
+  g_prof.resolve();
+  if (launches) *launches = g_prof.n[kclass];
+  if (total_ms) *total_ms = g_prof.ms[kclass];
+  return ATB_OK;
+}
+extern "C" int atb_launch_count(long* n) {
+  if (!n) return fail(ATB_ERR_INVALID, "null argument");
+  *n = g_prof.launches_total;
+  return ATB_OK;
+}
+
+extern "C" int atb_probe_fp64_peak(double* tflops, void* stream) {
+  if (!tflops) return fail(ATB_ERR_INVALID, "null argument");
+  *tflops = probe_fp64_tflops((cudaStream_t)stream);
+  return check_launch("fp64 probe");
+}
+
+// =============================================================== solvers
+struct atb_solver {
+  int kind = 0;
+  atb_op* rhs = nullptr;
+  atb_op* lin = nullptr;
+  atb_op* any = nullptr;
+  double dt = 0, time = 0, gamma_r = 1;
+  int split_rhs = 1;
+  int ns = 0;
+  size_t stride = 0;
+  std::vector<double> rka, rkb, rkc, rkb_full;
+  double exa[3][3], ima[3][3], exb[3], imb[3], exc[3], imc[3];
+  double* dq = nullptr;  // LSRK: dq; RLSRK: dq
+  double* qB = nullptr;  // LSRK double buffer; RLSRK: q0
+  double* kb = nullptr;  // RLSRK: k
+  double* Qs = nullptr;  // ARK: 2 stage states
+  double* exK = nullptr; // ARK: 3
+  double* imK = nullptr; // ARK: 3
+  // banded operator
+  LineMap M{};
+  int* d_e0 = nullptr;
+  double* band = nullptr;
+  double* blk = nullptr;
+  int ld = 0;
+};
+
+namespace {
+
+void solver_free(atb_solver* s) {
+  cudaFree(s->dq);
+  cudaFree(s->qB);
+  cudaFree(s->kb);
+  cudaFree(s->Qs);
+  cudaFree(s->exK);
+  cudaFree(s->imK);
+  cudaFree(s->d_e0);
+  cudaFree(s->band);
+  cudaFree(s->blk);
+  delete s;
+}
+
+void coeffs_lsrk54(atb_solver* s) {
+  // Carpenter-Kennedy LSRK(5,4) (src/odesolvers.jl:148-174), rationals rounded once
+  s->rka = {0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
+            -3550918686646.0 / 2091501179385.0, -1275806237668.0 / 842570457699.0};
+  s->rkb = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+            1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+            2277821191437.0 / 14882151754819.0};
+  s->rkc = {0.0, 1432997174477.0 / 9575080441755.0, 2526269341429.0 / 6820363962896.0,
+            2006345519317.0 / 3224310063776.0, 2802321613138.0 / 2924317926251.0};
+}
+
+void coeffs_lsrk144(atb_solver* s) {
+  // Niegemann-Diehl-Busch LSRK(14,4) (src/odesolvers.jl:176-229)
+  s->rka = {0, -0.7188012108672410, -0.7785331173421570, -0.0053282796654044, -0.8552979934029281,
+            -3.9564138245774565, -1.5780575380587385, -2.0837094552574054, -0.7483334182761610,
+            -0.7032861106563359, 0.0013917096117681, -0.0932075369637460, -0.9514200470875948,
+            -7.1151571693922548};
+  s->rkb = {0.0367762454319673, 0.3136296607553959, 0.1531848691869027, 0.0030097086818182,
+            0.3326293790646110, 0.2440251405350864, 0.3718879239592277, 0.6204126221582444,
+            0.1524043173028741, 0.0760894927419266, 0.0077604214040978, 0.0024647284755382,
+            0.0780348340049386, 5.5059777270269628};
+  s->rkc = {0, 0.0367762454319673, 0.1249685262725025, 0.2446177702277698, 0.2476149531070420,
+            0.2969311120382472, 0.3978149645802642, 0.5270854589440328, 0.6981269994175695,
+            0.8190890835352128, 0.8527059887098624, 0.8604711817462826, 0.8627060376969976,
+            0.8734213127600976};
+}
+
+int copy_field(double* const* dst, const double* const* src, int ns, size_t n, cudaStream_t st) {
+  for (int s = 0; s < ns; ++s)
+    CK(cudaMemcpyAsync(dst[s], src[s], n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  return ATB_OK;
+}
+
+int build_band(atb_solver* s, cudaStream_t st) {
+  atb_op* L = s->lin;
+  const int dim = L->dim, Nq = L->Nq, ns = L->ns;
+  if (!(L->dirs == (1 << (dim - 1))))
+    return fail(ATB_ERR_INVALID, "the implicit operator must act along the last dimension only");
+  LineMap& M = s->M;
+  M.Nq = Nq;
+  M.ns = ns;
+  M.Np = L->Np;
+  M.nh = L->Np / Nq;
+  M.KV = L->Kd[dim - 1];
+  M.KH = L->K / M.KV;
+  M.nlines = M.KH * M.nh;
+  M.nunk = M.KV * Nq * ns;
+  M.bw = Nq * ns - 1;
+  M.stride = L->stride();
+  M.stacked = L->stacked;
+  if (M.bw >= 64) return fail(ATB_ERR_INVALID, "banded bandwidth too large");
+  // element index of the bottom element of each horizontal stack
+  std::vector<int> e0(M.nlines);
+  for (int eh = 0; eh < M.KH; ++eh) {
+    int idx[3] = {0, 0, 0}, r = eh;
+    for (int d = 0; d < dim - 1; ++d) { idx[d] = r % L->Kd[d]; r /= L->Kd[d]; }
+    idx[dim - 1] = 0;
+    int eb = L->elem_of(idx);
+    for (int hn = 0; hn < M.nh; ++hn) e0[eh * M.nh + hn] = eb;
+  }
+  M.estep = L->stacked ? 1 : M.KH;
+  int rc;
+  if ((rc = dalloc(&s->d_e0, (size_t)M.nlines))) return rc;
+  CK(cudaMemcpy(s->d_e0, e0.data(), e0.size() * sizeof(int), cudaMemcpyHostToDevice));
+  M.e0 = s->d_e0;
+  const int W = 2 * M.bw + 1;
+  const size_t bandn = (size_t)M.nlines * M.nunk * W;
+  if ((rc = dalloc(&s->band, bandn))) return rc;
+  CK(cudaMemsetAsync(s->band, 0, bandn * sizeof(double), st));
+  double *P = nullptr, *LP = nullptr;
+  const size_t fsz = (size_t)ns * M.stride;
+  if ((rc = dalloc(&P, fsz))) return rc;
+  if ((rc = dalloc(&LP, fsz))) { cudaFree(P); return rc; }
+  double *pp[5], *lp[5];
+  field_ptrs(P, ns, M.stride, pp);
+  field_ptrs(LP, ns, M.stride, lp);
+  CK(cudaMemsetAsync(P, 0, fsz * sizeof(double), st));
+  for (int c = 0; c < W && rc == ATB_OK; ++c) {
+    launch_probe_fill(M, c, pp, st);
+    rc = run_tendency(L, EPI_SET, pp, lp, nullptr, 0, 0, st);
+    if (!rc) launch_band_extract(M, c, lp, s->band, st);
+  }
+  cudaFree(P);
+  cudaFree(LP);
+  if (rc) return rc;
+  // one factor per distinct column: the probed operators of a horizontally
+  // uniform problem are bitwise identical in every column -> keep one copy
+  int* d_nd = nullptr;
+  if ((rc = dalloc(&d_nd, 1))) return rc;
+  CK(cudaMemsetAsync(d_nd, 0, sizeof(int), st));
+  launch_band_compare(M, s->band, d_nd, st);
+  int nd = 0;
+  CK(cudaMemcpyAsync(&nd, d_nd, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  cudaFree(d_nd);
+  const double scale = -s->dt * s->ima[2][2];  // M = I - dt a_ii L (src/odesolvers.jl:264-268)
+  if (nd == 0) {
+    double* one = nullptr;
+    if ((rc = dalloc(&one, (size_t)M.nunk * 2 * (M.bw + 1)))) return rc;
+    launch_band_compact(M, s->band, one, st);
+    launch_band_factor(M.nunk, M.bw, 1, one, 2 * (M.bw + 1), 1, scale, st);
+    CK(cudaStreamSynchronize(st));
+    cudaFree(s->band);
+    s->band = one;
+    s->ld = 1;
+    // per-element inverses for the block-parallel solve
+    const int BW1 = M.bw + 1;
+    if ((rc = dalloc(&s->blk, (size_t)M.KV * 4 * BW1 * BW1))) return rc;
+    launch_block_prep(s->band, M.KV, BW1, s->blk, st);
+    CK(cudaStreamSynchronize(st));
+  } else {
+    launch_band_factor(M.nunk, M.bw, M.nlines, s->band, W, M.nlines, scale, st);
+    s->ld = M.nlines;
+  }
+  if ((rc = check_launch("band factor"))) return rc;
+  return ATB_OK;
+}
+
+// ------------------------------------------------------------ one step
+int lsrk_steps(atb_solver* s, double* const* q, int nsteps, cudaStream_t st) {
+  atb_op* op = s->rhs;
+  double *dq[5], *qb[5], *cur[5], *oth[5];
+  field_ptrs(s->dq, s->ns, s->stride, dq);
+  field_ptrs(s->qB, s->ns, s->stride, qb);
+  for (int k = 0; k < 5; ++k) { cur[k] = q[k < s->ns ? k : 0]; oth[k] = qb[k]; }
+  bool in_user = true;
+  for (int n = 0; n < nsteps; ++n) {
+    for (size_t st_ = 0; st_ < s->rka.size(); ++st_) {
+      int rc = run_tendency(op, EPI_LSRK, cur, dq, oth, s->rka[st_], s->rkb[st_] * s->dt, st);
+      if (rc) return rc;
+      for (int k = 0; k < 5; ++k) std::swap(cur[k], oth[k]);
+      in_user = !in_user;
+    }
+    s->time += s->dt;
+  }
+  if (!in_user) return copy_field(q, cur, s->ns, s->stride, st);
+  return ATB_OK;
+}
+
+int rlsrk_step(atb_solver* s, double* const* q, cudaStream_t st) {
+  atb_op* op = s->rhs;
+  double *dq[5], *q0[5], *k[5];
+  field_ptrs(s->dq, s->ns, s->stride, dq);
+  field_ptrs(s->qB, s->ns, s->stride, q0);
+  field_ptrs(s->kb, s->ns, s->stride, k);
+  int rc = copy_field(q0, q, s->ns, s->stride, st);
+  if (rc) return rc;
+  double eta0 = 0, deta = -0.0;
+  if ((rc = atb_entropyintegral(op, q0, &eta0, st))) return rc;
+  for (size_t i = 0; i < s->rka.size(); ++i) {
+    if ((rc = run_tendency(op, EPI_RLSRK, q, k, dq, s->rka[i], 0, st))) return rc;
+    double ep = 0;
+    if ((rc = atb_entropyproduct(op, q, k, &ep, st))) return rc;
+    deta = deta + s->rkb_full[i] * s->dt * ep;
+    Axpy A{};
+    A.ns = s->ns;
+    A.n = s->stride;
+    A.c = s->rkb[i] * s->dt;
+    for (int c = 0; c < 5; ++c) { A.x[c] = q[c < s->ns ? c : 0]; A.y[c] = dq[c]; A.out[c] = q[c < s->ns ? c : 0]; }
+    ProfScope ps(ATB_PROF_COMBINE, st);
+    launch_axpy(A, st);
+    if ((rc = check_launch("axpy"))) return rc;
+  }
+  // k = q - q0
+  {
+    Axpy A{};
+    A.ns = s->ns;
+    A.n = s->stride;
+    A.c = -1.0;
+    for (int c = 0; c < 5; ++c) { A.x[c] = q[c < s->ns ? c : 0]; A.y[c] = q0[c]; A.out[c] = k[c]; }
+    ProfScope ps(ATB_PROF_COMBINE, st);
+    launch_axpy(A, st);
+  }
+  auto setq = [&](double g) {
+    Axpy A{};
+    A.ns = s->ns;
+    A.n = s->stride;
+    A.c = g;
+    for (int c = 0; c < 5; ++c) { A.x[c] = q0[c]; A.y[c] = k[c]; A.out[c] = q[c < s->ns ? c : 0]; }
+    {
+      ProfScope ps(ATB_PROF_COMBINE, st);
+      launch_axpy(A, st);
+    }
+    return check_launch("axpy");
+  };
+  auto resid = [&](double g, double* r) {
+    int e = setq(g);
+    if (e) return e;
+    double eta = 0;
+    e = atb_entropyintegral(op, q, &eta, st);
+    *r = eta - eta0 - g * deta;
+    return e;
+  };
+  auto jac = [&](double g, double* J) {
+    int e = setq(g);
+    if (e) return e;
+    double ep = 0;
+    e = atb_entropyproduct(op, q, k, &ep, st);
+    *J = ep - deta;
+    return e;
+  };
+  // NLsolve trust region (autoscale, factor 1, eta 1e-4, ftol 10 eps, xtol 0)
+  const double ftol = 10 * 2.220446049250313e-16;
+  double g = s->gamma_r, r = 0;
+  if ((rc = resid(g, &r))) return rc;
+  if (!(std::fabs(r) <= ftol)) {
+    double J = 0;
+    if ((rc = jac(g, &J))) return rc;
+    double Dsc = std::fabs(J) > 0 ? std::fabs(J) : 1.0;
+    double delta = std::fabs(Dsc * g) > 0 ? std::fabs(Dsc * g) : 1.0;
+    for (int it = 0; it < 1000; ++it) {
+      if (!(J != 0) || !std::isfinite(J)) break;
+      double p = -r / J;
+      if (std::fabs(Dsc * p) > delta) p = (p > 0 ? delta : -delta) / Dsc;
+      double gn = g + p, rn = 0;
+      if ((rc = resid(gn, &rn))) return rc;
+      double rp = r + J * p;
+      double rho = (r * r - rn * rn) / (r * r - rp * rp);
+      bool conv = false;
+      if (rho > 1e-4) {
+        g = gn;
+        r = rn;
+        if ((rc = jac(g, &J))) return rc;
+        Dsc = std::max(0.1 * Dsc, std::fabs(J));
+        conv = (p == 0) || std::fabs(r) <= ftol;
+      }
+      double np_ = std::fabs(Dsc * p);
+      if (rho < 0.1)
+        delta = delta / 2;
+      else if (rho >= 0.9)
+        delta = 2 * np_;
+      else if (rho >= 0.5)
+        delta = std::max(delta, 2 * np_);
+      if (conv || !(delta > 0)) break;
+    }
+  }
+  s->gamma_r = g;
+  if ((rc = setq(g))) return rc;
+  s->time += s->dt;
+  return ATB_OK;
+}
+
+int ark_step(atb_solver* s, double* const* q, cudaStream_t st) {
+  const int ns = s->ns;
+  const size_t n = s->stride;
+  double *Q[3][5], *ex[3][5], *im[3][5];
+  for (int k = 0; k < 5; ++k) Q[0][k] = q[k < ns ? k : 0];
+  field_ptrs(s->Qs, ns, n, Q[1]);
+  field_ptrs(s->Qs + (size_t)ns * n, ns, n, Q[2]);
+  for (int i = 0; i < 3; ++i) {
+    field_ptrs(s->exK + (size_t)i * ns * n, ns, n, ex[i]);
+    field_ptrs(s->imK + (size_t)i * ns * n, ns, n, im[i]);
+  }
+  auto eval = [&](int i) -> int {
+    int rc;
+    if (s->rhs) {
+      if ((rc = run_tendency(s->rhs, EPI_SET, Q[i], ex[i], nullptr, 0, 0, st))) return rc;
+    } else {
+      for (int c = 0; c < ns; ++c) CK(cudaMemsetAsync(ex[i][c], 0, n * sizeof(double), st));
+    }
+    if (s->lin) {
+      if (!s->split_rhs)
+        rc = run_tendency(s->lin, EPI_SUBOUT2, Q[i], im[i], ex[i], 0, 0, st);
+      else
+        rc = run_tendency(s->lin, EPI_SET, Q[i], im[i], nullptr, 0, 0, st);
+      if (rc) return rc;
+    } else {
+      for (int c = 0; c < ns; ++c) CK(cudaMemsetAsync(im[i][c], 0, n * sizeof(double), st));
+    }
+    return ATB_OK;
+  };
+  int rc = eval(0);
+  if (rc) return rc;
+  for (int i = 1; i < 3; ++i) {
+    if (s->lin) {
+      BandSolve B{};
+      B.M = s->M;
+      B.band = s->band;
+      B.blk = s->blk;
+      B.ld = s->ld;
+      B.npairs = i;
+      B.dt = s->dt;
+      for (int k = 0; k < i; ++k) {
+        B.a[k] = s->exa[i][k];
+        B.b[k] = s->ima[i][k];
+        for (int c = 0; c < 5; ++c) { B.ex[k][c] = ex[k][c]; B.im[k][c] = im[k][c]; }
+      }
+      for (int c = 0; c < 5; ++c) { B.q[c] = q[c < ns ? c : 0]; B.out[c] = Q[i][c]; }
+      {
+        ProfScope ps(ATB_PROF_BAND, st);
+        launch_band_solve(B, st);
+      }
+      if ((rc = check_launch("band solve"))) return rc;
+    } else {
+      LinComb C{};
+      C.ns = ns;
+      C.n = n;
+      C.npairs = i;
+      C.dt = s->dt;
+      for (int k = 0; k < i; ++k) {
+        C.a[k] = s->exa[i][k];
+        C.b[k] = s->ima[i][k];
+        for (int c = 0; c < 5; ++c) { C.X[k][c] = ex[k][c]; C.Y[k][c] = im[k][c]; }
+      }
+      for (int c = 0; c < 5; ++c) { C.base[c] = q[c < ns ? c : 0]; C.out[c] = Q[i][c]; }
+      {
+        ProfScope ps(ATB_PROF_COMBINE, st);
+        launch_lincomb(C, st);
+      }
+      if ((rc = check_launch("lincomb"))) return rc;
+    }
+    if ((rc = eval(i))) return rc;
+  }
+  LinComb C{};
+  C.ns = ns;
+  C.n = n;
+  C.npairs = 3;
+  C.dt = s->dt;
+  for (int k = 0; k < 3; ++k) {
+    C.a[k] = s->exb[k];
+    C.b[k] = s->imb[k];
+    for (int c = 0; c < 5; ++c) { C.X[k][c] = ex[k][c]; C.Y[k][c] = im[k][c]; }
+  }
+  for (int c = 0; c < 5; ++c) { C.base[c] = q[c < ns ? c : 0]; C.out[c] = q[c < ns ? c : 0]; }
+  {
+    ProfScope ps(ATB_PROF_COMBINE, st);
+    launch_lincomb(C, st);
+  }
+  if ((rc = check_launch("lincomb"))) return rc;
+  s->time += s->dt;
+  return ATB_OK;
+}
+
+int do_steps(atb_solver* s, double* const* q, int nsteps, cudaStream_t st) {
+  if (s->kind <= ATB_LSRK144) return lsrk_steps(s, q, nsteps, st);
+  for (int i = 0; i < nsteps; ++i) {
+    int rc = (s->kind <= ATB_RLSRK144) ? rlsrk_step(s, q, st) : ark_step(s, q, st);
+    if (rc) return rc;
+  }
+  return ATB_OK;
+}
+
+}  // namespace
+
+extern "C" int atb_solver_create(int kind, atb_op* rhs, atb_op* linrhs, double dt, double t0, int split_rhs,
+                                 int paperversion, atb_solver** out) {
+  if (!out) return fail(ATB_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (kind < ATB_LSRK54 || kind > ATB_ARK23) return fail(ATB_ERR_INVALID, "unknown solver kind %d", kind);
+  if (kind != ATB_ARK23 && (!rhs || linrhs)) return fail(ATB_ERR_INVALID, "explicit solvers take rhs only");
+  if (kind == ATB_ARK23 && !rhs && !linrhs) return fail(ATB_ERR_INVALID, "ARK23 needs rhs or linrhs");
+  atb_op* any = rhs ? rhs : linrhs;
+  if (rhs && linrhs && (rhs->ns != linrhs->ns || rhs->K != linrhs->K || rhs->Np != linrhs->Np))
+    return fail(ATB_ERR_INVALID, "rhs and linrhs act on different fields");
+  atb_solver* s = new atb_solver();
+  s->kind = kind;
+  s->rhs = rhs;
+  s->lin = linrhs;
+  s->any = any;
+  s->dt = dt;
+  s->time = t0;
+  s->split_rhs = split_rhs;
+  if (linrhs) linrhs->prof_class = ATB_PROF_TEND_LIN;
+  s->ns = any->ns;
+  s->stride = any->stride();
+  const size_t fsz = (size_t)s->ns * s->stride;
+  int rc = ATB_OK;
+  if (kind <= ATB_RLSRK144) {
+    if (kind == ATB_LSRK54 || kind == ATB_RLSRK54)
+      coeffs_lsrk54(s);
+    else
+      coeffs_lsrk144(s);
+    if ((rc = dalloc(&s->dq, fsz)) || (rc = dalloc(&s->qB, fsz))) { solver_free(s); return rc; }
+    cudaMemset(s->dq, 0, fsz * sizeof(double));
+    if (kind >= ATB_RLSRK54) {
+      if ((rc = dalloc(&s->kb, fsz))) { solver_free(s); return rc; }
+      const size_t nst = s->rkb.size();
+      s->rkb_full.assign(nst, 0.0);
+      s->rkb_full[nst - 1] = s->rkb[nst - 1];
+      for (int i = (int)nst - 2; i >= 0; --i) s->rkb_full[i] = s->rka[i + 1] * s->rkb_full[i + 1] + s->rkb[i];
+    }
+  } else {
+    // ARK23, Giraldo-Kelly-Constantinescu 2013 (src/odesolvers.jl:284-309)
+    const double r2 = std::sqrt(2.0);
+    const double a32 = paperversion ? (3 + 2 * r2) / 6 : 0.5;
+    const double exa[3][3] = {{0, 0, 0}, {2 - r2, 0, 0}, {1 - a32, a32, 0}};
+    const double ima[3][3] = {{0, 0, 0}, {1 - 1 / r2, 1 - 1 / r2, 0}, {1 / (2 * r2), 1 / (2 * r2), 1 - 1 / r2}};
+    const double exb[3] = {1 / (2 * r2), 1 / (2 * r2), 1 - 1 / r2};
+    const double exc[3] = {0, 2 - r2, 1};
+    std::memcpy(s->exa, exa, sizeof(exa));
+    std::memcpy(s->ima, ima, sizeof(ima));
+    std::memcpy(s->exb, exb, sizeof(exb));
+    std::memcpy(s->imb, exb, sizeof(exb));
+    std::memcpy(s->exc, exc, sizeof(exc));
+    std::memcpy(s->imc, exc, sizeof(exc));
+    if ((rc = dalloc(&s->Qs, 2 * fsz)) || (rc = dalloc(&s->exK, 3 * fsz)) || (rc = dalloc(&s->imK, 3 * fsz))) {
+      solver_free(s);
+      return rc;
+    }
+    if (linrhs && (rc = build_band(s, 0))) {
+      solver_free(s);
+      return rc;
+    }
+  }
+  if ((rc = check_launch("solver create"))) { solver_free(s); return rc; }
+  *out = s;
+  return ATB_OK;
+}
+
+extern "C" int atb_solver_destroy(atb_solver* s) {
+  if (s) solver_free(s);
+  return ATB_OK;
+}
+
+extern "C" int atb_solver_step(atb_solver* s, double* const* q, int nsteps, void* stream) {
+  if (!s || !q || nsteps < 0) return fail(ATB_ERR_INVALID, "bad argument");
+  return do_steps(s, q, nsteps, (cudaStream_t)stream);
+}
+
+extern "C" int atb_solve(atb_solver* s, double* const* q, double timeend, int adjust_final, int* steps_out,
+                         void* stream) {
+  if (!s || !q) return fail(ATB_ERR_INVALID, "bad argument");
+  int step = 0;
+  bool finalstep = false;
+  while (true) {
+    ++step;
+    const double time = s->time;
+    if (time + s->dt >= timeend) {
+      if (adjust_final) s->dt = timeend - time;
+      finalstep = true;
+    }
+    int rc = do_steps(s, q, 1, (cudaStream_t)stream);
+    if (rc) return rc;
+    if (finalstep) break;
+  }
+  if (steps_out) *steps_out = step;
+  return ATB_OK;
+}
+
+extern "C" int atb_solver_get(const atb_solver* s, double* time, double* dt, double* gamma) {
+  if (!s) return fail(ATB_ERR_INVALID, "null solver");
+  if (time) *time = s->time;
+  if (dt) *dt = s->dt;
+  if (gamma) *gamma = s->gamma_r;
+  return ATB_OK;
+}
+
+extern "C" int atb_solver_set_dt(atb_solver* s, double dt) {
+  if (!s) return fail(ATB_ERR_INVALID, "null solver");
+  if (s->kind == ATB_ARK23 && s->lin && dt != s->dt)
+    return fail(ATB_ERR_INVALID, "ARK23 factors I - dt a L for a fixed dt");
+  s->dt = dt;
+  return ATB_OK;
+}

@@ -1,0 +1,259 @@
+// Law-independent kernels (see atb_generic.cuh).
+#include "atb_generic.cuh"
+
+#include <math.h>
+
+namespace atb {
+
+// ------------------------------------------------------------ elementwise
+__global__ void lincomb_kernel(const LinComb C) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < C.n; i += stride) {
+    for (int s = 0; s < C.ns; ++s) {
+      double acc = C.base[s][i];
+      for (int k = 0; k < C.npairs; ++k) acc = acc + C.dt * (C.a[k] * C.X[k][s][i] + C.b[k] * C.Y[k][s][i]);
+      C.out[s][i] = acc;
+    }
+  }
+}
+
+static int grid_for(size_t n, int threads) {
+  size_t g = (n + threads - 1) / threads;
+  if (g > 148 * 32) g = 148 * 32;  // grid-stride: a few waves over 148 SMs
+  return (int)(g < 1 ? 1 : g);
+}
+
+void launch_lincomb(const LinComb& C, cudaStream_t st) {
+  lincomb_kernel<<<grid_for(C.n, 256), 256, 0, st>>>(C);
+}
+
+__global__ void axpy_kernel(const Axpy A) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += stride)
+    for (int s = 0; s < A.ns; ++s) A.out[s][i] = A.x[s][i] + A.c * A.y[s][i];
+}
+
+void launch_axpy(const Axpy& A, cudaStream_t st) { axpy_kernel<<<grid_for(A.n, 256), 256, 0, st>>>(A); }
+
+// ------------------------------------------------------------ band probe
+__device__ __forceinline__ size_t line_gid(const LineMap& M, int line, int ev, int kv) {
+  const int eh = line / M.nh, hn = line - eh * M.nh;
+  (void)eh;
+  const int e = M.e0[line] + ev * M.estep;
+  return (size_t)e * M.Np + hn + (size_t)M.nh * kv;
+}
+
+// Probe vector for colour c: 1 at every unknown u with u mod W == c.
+__global__ void probe_fill_kernel(const LineMap M, int color, double* P0, double* P1, double* P2, double* P3,
+                                  double* P4) {
+  double* P[5] = {P0, P1, P2, P3, P4};
+  const int W = 2 * M.bw + 1;
+  const size_t total = (size_t)M.nlines * M.nunk;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int line = (int)(t % M.nlines);
+    const int u = (int)(t / M.nlines);
+    const int s = u % M.ns, kvg = u / M.ns;
+    const int ev = kvg / M.Nq, kv = kvg - ev * M.Nq;
+    P[s][line_gid(M, line, ev, kv)] = (u % W == color) ? 1.0 : 0.0;
+  }
+}
+
+void launch_probe_fill(const LineMap& M, int color, double* const* P, cudaStream_t st) {
+  size_t total = (size_t)M.nlines * M.nunk;
+  double* p[5] = {P[0], P[0], P[0], P[0], P[0]};
+  for (int s = 0; s < M.ns; ++s) p[s] = P[s];
+  probe_fill_kernel<<<grid_for(total, 256), 256, 0, st>>>(M, color, p[0], p[1], p[2], p[3], p[4]);
+}
+
+__global__ void band_extract_kernel(const LineMap M, int color, const double* L0, const double* L1,
+                                    const double* L2, const double* L3, const double* L4, double* band) {
+  const double* LP[5] = {L0, L1, L2, L3, L4};
+  const int W = 2 * M.bw + 1;
+  const size_t total = (size_t)M.nlines * M.nunk;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int line = (int)(t % M.nlines);
+    const int r = (int)(t / M.nlines);
+    int delta = ((color - r) % W + W) % W;
+    int j = delta <= M.bw ? r + delta : r + delta - W;
+    if (j < 0 || j >= M.nunk) continue;
+    const int s = r % M.ns, kvg = r / M.ns;
+    const int ev = kvg / M.Nq, kv = kvg - ev * M.Nq;
+    band[((size_t)r * W + (j - r + M.bw)) * M.nlines + line] = LP[s][line_gid(M, line, ev, kv)];
+  }
+}
+
+void launch_band_extract(const LineMap& M, int color, const double* const* LP, double* band, cudaStream_t st) {
+  size_t total = (size_t)M.nlines * M.nunk;
+  const double* p[5] = {LP[0], LP[0], LP[0], LP[0], LP[0]};
+  for (int s = 0; s < M.ns; ++s) p[s] = LP[s];
+  band_extract_kernel<<<grid_for(total, 256), 256, 0, st>>>(M, color, p[0], p[1], p[2], p[3], p[4], band);
+}
+
+// M = I + scale * A, then LU without pivoting, in place (one thread per
+// matrix).  Entry (i, j) lives at band[(i * rs + (j - i + bw)) * ld + l].
+__global__ void band_factor_kernel(int n, int bw, int nl, double* band, int rs, int ld, double scale) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= nl) return;
+  const int W = 2 * bw + 1;
+  auto at = [&](int i, int j) -> double& { return band[((size_t)i * rs + (j - i + bw)) * ld + l]; };
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < W; ++k) {
+      double& v = band[((size_t)i * rs + k) * ld + l];
+      v = v * scale;
+    }
+  for (int i = 0; i < n; ++i) at(i, i) += 1.0;
+  for (int k = 0; k < n; ++k) {
+    const double piv = at(k, k);
+    const int iend = min(k + bw, n - 1);
+    for (int i = k + 1; i <= iend; ++i) {
+      const double lik = at(i, k) / piv;
+      at(i, k) = lik;
+      for (int j = k + 1; j <= iend; ++j) at(i, j) = at(i, j) - lik * at(k, j);
+    }
+  }
+}
+
+void launch_band_factor(int n, int bw, int nl, double* band, int rs, int ld, double scale, cudaStream_t st) {
+  band_factor_kernel<<<(nl + 63) / 64, 64, 0, st>>>(n, bw, nl, band, rs, ld, scale);
+}
+
+__global__ void band_compact_kernel(const LineMap M, const double* band, double* out) {
+  const int W = 2 * M.bw + 1, rs = 2 * (M.bw + 1);
+  const size_t total = (size_t)M.nunk * rs;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const size_t r = t / rs, k = t - r * rs;
+    out[t] = (k < (size_t)W) ? band[(r * W + k) * M.nlines] : 0.0;
+  }
+}
+
+void launch_band_compact(const LineMap& M, const double* band, double* out, cudaStream_t st) {
+  size_t total = (size_t)M.nunk * 2 * (M.bw + 1);
+  band_compact_kernel<<<grid_for(total, 256), 256, 0, st>>>(M, band, out);
+}
+
+__global__ void band_compare_kernel(const LineMap M, const double* band, int* ndiff) {
+  const int W = 2 * M.bw + 1;
+  const size_t total = (size_t)M.nlines * M.nunk * W;
+  int local = 0;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const size_t line = t % M.nlines, idx = t / M.nlines;
+    const double a = band[idx * M.nlines + line], b = band[idx * M.nlines];
+    // bitwise comparison (NaN-safe)
+    if (__double_as_longlong(a) != __double_as_longlong(b)) local = 1;
+  }
+  if (local) atomicAdd(ndiff, 1);
+}
+
+void launch_band_compare(const LineMap& M, const double* band, int* ndiff, cudaStream_t st) {
+  size_t total = (size_t)M.nlines * M.nunk * (2 * M.bw + 1);
+  band_compare_kernel<<<grid_for(total, 256), 256, 0, st>>>(M, band, ndiff);
+}
+
+// Generic fallback (one thread per vertical line, per-line factors in the
+// line-fastest layout or any block size): forms the ARK right-hand side on the
+// fly, forward substitution with L (unit diagonal), back substitution with U,
+// sliding window of the last 64 values (bw = Nq*ns - 1 <= 39).  The fast path
+// for a shared factor is band_solve_shared in atb_band.cu.
+constexpr int WIN = 64;
+__global__ void __launch_bounds__(128) band_solve_generic_kernel(const BandSolve B) {
+  const LineMap& M = B.M;
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= M.nlines) return;
+  const int n = M.nunk, bw = M.bw, W = 2 * bw + 1, ns = M.ns, Nq = M.Nq;
+  const int ld = B.ld;
+  const int fl = (ld == 1) ? 0 : l;
+  const int rs = (ld == 1) ? W + 1 : W;  // compact shared factor: padded rows
+  const double* __restrict__ band = B.band;
+  double win[WIN];
+  // forward
+  int s = 0, kv = 0, ev = 0;
+  for (int r = 0; r < n; ++r) {
+    const size_t g = line_gid(M, l, ev, kv);
+    double acc = B.q[s][g];
+    for (int k = 0; k < B.npairs; ++k) acc = acc + B.dt * (B.a[k] * B.ex[k][s][g] + B.b[k] * B.im[k][s][g]);
+    const int j0 = r - bw > 0 ? r - bw : 0;
+    const double* row = band + ((size_t)r * rs - r + bw) * ld + fl;
+    for (int j = j0; j < r; ++j) acc = acc - row[(size_t)j * ld] * win[j & (WIN - 1)];
+    win[r & (WIN - 1)] = acc;
+    B.out[s][g] = acc;
+    if (++s == ns) { s = 0; if (++kv == Nq) { kv = 0; ++ev; } }
+  }
+  // backward
+  s = ns - 1; kv = Nq - 1; ev = M.KV - 1;
+  for (int r = n - 1; r >= 0; --r) {
+    const size_t g = line_gid(M, l, ev, kv);
+    double acc = B.out[s][g];
+    const int j1 = r + bw < n - 1 ? r + bw : n - 1;
+    const double* row = band + ((size_t)r * rs - r + bw) * ld + fl;
+    for (int j = r + 1; j <= j1; ++j) acc = acc - row[(size_t)j * ld] * win[j & (WIN - 1)];
+    const double x = acc / row[(size_t)r * ld];
+    win[r & (WIN - 1)] = x;
+    B.out[s][g] = x;
+    if (--s < 0) { s = ns - 1; if (--kv < 0) { kv = Nq - 1; --ev; } }
+  }
+}
+
+void launch_band_solve_generic(const BandSolve& B, cudaStream_t st) {
+  band_solve_generic_kernel<<<(B.M.nlines + 127) / 128, 128, 0, st>>>(B);
+}
+
+// ---------------------------------------------------------- reductions
+__global__ void red_finish_kernel(const double* partials, int nblocks, int linf, double* out5) {
+  const int k = threadIdx.x;
+  if (k >= 5) return;
+  double s = 0, c = 0;
+  for (int b = 0; b < nblocks; ++b) {
+    const double x = partials[b * 5 + k];
+    if (linf) {
+      s = fmax(s, x);
+    } else {
+      const double t = s + x;
+      c += (fabs(s) >= fabs(x)) ? (s - t) + x : (x - t) + s;
+      s = t;
+    }
+  }
+  out5[k] = s + c;
+}
+
+void launch_red_finish(const double* partials, int nblocks, int linf, double* out5, cudaStream_t st) {
+  red_finish_kernel<<<1, 32, 0, st>>>(partials, nblocks, linf, out5);
+}
+
+// ------------------------------------------------------------ FP64 probe
+__global__ void fp64_probe_kernel(double* out, int iters, double seed) {
+  double a0 = seed + threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6,
+         a7 = a0 + 7;
+  const double m = 0.999999, c = 1e-7;
+  for (int i = 0; i < iters; ++i) {
+    a0 = fma(a0, m, c); a1 = fma(a1, m, c); a2 = fma(a2, m, c); a3 = fma(a3, m, c);
+    a4 = fma(a4, m, c); a5 = fma(a5, m, c); a6 = fma(a6, m, c); a7 = fma(a7, m, c);
+  }
+  double r = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  if (r == 12345.678) out[0] = r;  // keeps the loop alive; practically never taken
+}
+
+double probe_fp64_tflops(cudaStream_t st) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  double* out = nullptr;
+  if (cudaMalloc(&out, sizeof(double)) != cudaSuccess) return -1;
+  const int threads = 512, blocks = sms * 4, iters = 1 << 14;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  fp64_probe_kernel<<<blocks, threads, 0, st>>>(out, 256, 1.0);  // warm-up
+  cudaEventRecord(a, st);
+  fp64_probe_kernel<<<blocks, threads, 0, st>>>(out, iters, 1.0);
+  cudaEventRecord(b, st);
+  cudaEventSynchronize(b);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(out);
+  const double flops = 2.0 * 8.0 * (double)iters * threads * blocks;
+  return flops / (ms * 1e-3) / 1e12;
+}
+
+}  // namespace atb

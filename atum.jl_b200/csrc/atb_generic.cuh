@@ -1,0 +1,75 @@
+// Law-independent kernels: stage linear combinations, the vertical-column
+// banded operator (probe assembly, no-pivot LU, batched solve fused with the
+// ARK right-hand-side combination), reduction finalisation and the FP64 probe.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+namespace atb {
+
+// out = base + dt * sum_k (a_k X_k + b_k Y_k), accumulated in k order like
+// `Qhat .+= dt .* (a .* ex_K[k] .+ at .* im_K[k])` (src/odesolvers.jl:346-349)
+// and the final update (src/odesolvers.jl:382-384).
+struct LinComb {
+  int ns, npairs;
+  size_t n;
+  double dt;
+  double a[3], b[3];
+  const double* base[5];
+  const double* X[3][5];
+  const double* Y[3][5];
+  double* out[5];
+};
+void launch_lincomb(const LinComb& C, cudaStream_t st);
+
+// out = x + c * y  (per component)
+struct Axpy {
+  int ns;
+  size_t n;
+  double c;
+  const double* x[5];
+  const double* y[5];
+  double* out[5];
+};
+void launch_axpy(const Axpy& A, cudaStream_t st);
+
+// Vertical lines of nodes: line l = eh * nh + hn (horizontal element stack eh,
+// horizontal node hn); unknown u = (ev * Nq + kv) * ns + s.
+struct LineMap {
+  int nlines, nunk, bw, Nq, ns, nh, KV, Np;
+  int stacked, KH;
+  size_t stride;
+  const int* e0;  // nlines: element index of the bottom element of the stack
+  int estep;      // element index step between vertically adjacent elements
+};
+
+void launch_probe_fill(const LineMap& M, int color, double* const* P, cudaStream_t st);
+// probed band layout (one matrix per line): band[(r * W + (j - r + bw)) * nlines + line]
+void launch_band_extract(const LineMap& M, int color, const double* const* LP, double* band, cudaStream_t st);
+void launch_band_compare(const LineMap& M, const double* band, int* ndiff, cudaStream_t st);
+// copy line 0 into a compact matrix with padded row stride rs = 2*(bw+1)
+void launch_band_compact(const LineMap& M, const double* band, double* out, cudaStream_t st);
+// M = I + scale*A then no-pivot LU in place; entry (i, j) at
+// band[(i * rs + (j - i + bw)) * ld + line], nl matrices
+void launch_band_factor(int n, int bw, int nl, double* band, int rs, int ld, double scale, cudaStream_t st);
+
+struct BandSolve {
+  LineMap M;
+  const double* band;
+  int ld;  // 1 when every column shares the factor (compact, row stride 2*(bw+1)), else nlines
+  // right-hand side: q + dt * sum_k (a_k ex_k + b_k im_k)
+  int npairs;
+  double dt, a[2], b[2];
+  const double* q[5];
+  const double* ex[2][5];
+  const double* im[2][5];
+  double* out[5];
+  const double* blk;  // per-element [L^-1 | G | U^-1 | H] blocks (shared factor), or null
+};
+void launch_band_solve(const BandSolve& B, cudaStream_t st);
+void launch_block_prep(const double* band, int KV, int BW1, double* blk, cudaStream_t st);
+
+void launch_red_finish(const double* partials, int nblocks, int linf, double* out5, cudaStream_t st);
+double probe_fp64_tflops(cudaStream_t st);
+
+}  // namespace atb

@@ -1,0 +1,21 @@
+// Tendency-kernel instantiations for LAW_ADV (one file per law so the
+// instantiations compile in parallel).
+#include "atb_tendency.cuh"
+#include "atb_reduce.cuh"
+namespace atb {
+template <> tend_launch_fn pick_launcher<LAW_ADV>(int dim, int vk) {
+  if (dim == 1 && vk == VK_WEAK) return tend_launch<LAW_ADV, 1, VK_WEAK>;
+  if (dim == 1 && vk == VK_CENTRAL) return tend_launch<LAW_ADV, 1, VK_CENTRAL>;
+  if (dim == 2 && vk == VK_WEAK) return tend_launch<LAW_ADV, 2, VK_WEAK>;
+  if (dim == 2 && vk == VK_CENTRAL) return tend_launch<LAW_ADV, 2, VK_CENTRAL>;
+  if (dim == 3 && vk == VK_WEAK) return tend_launch<LAW_ADV, 3, VK_WEAK>;
+  if (dim == 3 && vk == VK_CENTRAL) return tend_launch<LAW_ADV, 3, VK_CENTRAL>;
+  return nullptr;
+}
+template <> red_launch_fn pick_reducer<LAW_ADV>(int dim) {
+  if (dim == 1) return red_launch<LAW_ADV, 1>;
+  if (dim == 2) return red_launch<LAW_ADV, 2>;
+  if (dim == 3) return red_launch<LAW_ADV, 3>;
+  return nullptr;
+}
+}  // namespace atb

@@ -1,0 +1,120 @@
+"""Time steppers (host side of src/odesolvers.jl) driving the C ABI.
+
+``LSRK54(dg, q, dt)``, ``LSRK144``, ``RLSRK54``, ``RLSRK144`` and
+``ARK23(dg, lindg, q, dt; paperversion, split_rhs)`` construct solvers
+(src/odesolvers.jl:59-67,138-146,284-309); ``solve_(q, timeend, solver;
+after_step, after_stage, adjust_final)`` mirrors ``solve!``
+(src/odesolvers.jl:9-26): same step loop, same final-dt adjustment.
+
+Every stage runs on the GPU: LSRK stages are single fused tendency +
+write-back kernels, ARK23 stages are tendency kernels plus one batched
+vertical banded solve fused with the right-hand-side combination.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Callable, Optional
+
+from . import _lib
+
+__all__ = ["LSRK54", "LSRK144", "RLSRK54", "RLSRK144", "ARK23", "solve_", "Solver"]
+
+_KINDS = {"LSRK54": 0, "LSRK144": 1, "RLSRK54": 2, "RLSRK144": 3, "ARK23": 4}
+
+
+class Solver:
+    def __init__(self, kind: str, rhs, dt: float, t0: float = 0.0, linrhs=None, split_rhs: bool = True,
+                 paperversion: bool = False):
+        self.kind = kind
+        self.rhs = rhs
+        self.linrhs = linrhs
+        any_ = rhs if rhs is not None else linrhs
+        self.ns = any_.law.numberofstates
+        h = C.c_void_p()
+        _lib.check(_lib.lib().atb_solver_create(_KINDS[kind], rhs.device.h if rhs is not None else None,
+                                                linrhs.device.h if linrhs is not None else None, float(dt),
+                                                float(t0), int(bool(split_rhs)), int(bool(paperversion)),
+                                                C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h and _lib._LIB is not None:
+            _lib._LIB.atb_solver_destroy(h)
+            self.h = None
+
+    def _get(self):
+        t, dt, g = C.c_double(), C.c_double(), C.c_double()
+        _lib.check(_lib.lib().atb_solver_get(self.h, C.byref(t), C.byref(dt), C.byref(g)))
+        return t.value, dt.value, g.value
+
+    @property
+    def time(self) -> float:
+        return self._get()[0]
+
+    @property
+    def dt(self) -> float:
+        return self._get()[1]
+
+    @dt.setter
+    def dt(self, v: float):
+        _lib.check(_lib.lib().atb_solver_set_dt(self.h, float(v)))
+
+    @property
+    def gamma(self) -> float:
+        return self._get()[2]
+
+    def step(self, q, nsteps: int = 1, stream=None):
+        """``dostep!`` repeated ``nsteps`` times (no host synchronisation)."""
+        _lib.check(_lib.lib().atb_solver_step(self.h, _lib.field_ptrs(q, self.ns), int(nsteps),
+                                              _lib.stream_ptr(stream)))
+
+
+def LSRK54(rhs, q, dt, t0=0.0):
+    return Solver("LSRK54", rhs, dt, t0)
+
+
+def LSRK144(rhs, q, dt, t0=0.0):
+    return Solver("LSRK144", rhs, dt, t0)
+
+
+def RLSRK54(rhs, q, dt, t0=0.0):
+    return Solver("RLSRK54", rhs, dt, t0)
+
+
+def RLSRK144(rhs, q, dt, t0=0.0):
+    return Solver("RLSRK144", rhs, dt, t0)
+
+
+def ARK23(rhs, linrhs, q, dt, t0=0.0, paperversion=False, split_rhs=True):
+    return Solver("ARK23", rhs, dt, t0, linrhs=linrhs, split_rhs=split_rhs, paperversion=paperversion)
+
+
+def solve_(q, timeend: float, solver: Solver, after_step: Optional[Callable] = None,
+           after_stage: Optional[Callable] = None, adjust_final: bool = True, stream=None) -> int:
+    """``solve!(q, timeend, solver; after_step, after_stage, adjust_final)``.
+
+    Returns the number of steps.  ``after_step(step, time, q)`` runs on the
+    host after each step; the stage kernels are fused, so ``after_stage`` is
+    not supported.
+    """
+    if after_stage is not None:
+        raise NotImplementedError("after_stage callbacks: the stage update is fused into the tendency kernel")
+    if after_step is None:
+        steps = C.c_int()
+        _lib.check(_lib.lib().atb_solve(solver.h, _lib.field_ptrs(q, solver.ns), float(timeend),
+                                        int(bool(adjust_final)), C.byref(steps), _lib.stream_ptr(stream)))
+        return steps.value
+    step = 0
+    while True:
+        step += 1
+        time, dt, _ = solver._get()
+        final = False
+        if time + dt >= timeend:
+            if adjust_final:
+                solver.dt = timeend - time
+            final = True
+        solver.step(q, 1, stream)
+        after_step(step, time, q)
+        if final:
+            return step

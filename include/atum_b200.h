@@ -1,0 +1,159 @@
+/*
+ * atum_b200 — C ABI of the B200-native DGSEM tendency + time-stepping library
+ * (libatumb200.so, sm_100a).
+ *
+ * Each entry point replaces one call of the reference Atum.jl path; the
+ * reference location is given beside it (paths relative to the Atum.jl
+ * repository).  All functions return an int status (ATB_OK = 0, negative on
+ * error, message from atb_last_error()).  Nothing throws across the ABI.
+ * Handles are not thread-safe; distinct handles may be used from distinct
+ * threads.
+ *
+ * Field arguments are host arrays of Ns DEVICE pointers (the components of
+ * the reference's StructArray fieldarray), each component holding K*Np
+ * float64 values, node index i + Nq*(j + Nq*k) fastest, element slowest
+ * (src/dgsem.jl:251, q[ijk, e]).  Streams are cudaStream_t passed as void*
+ * (NULL = the legacy default stream).
+ */
+#ifndef ATUM_B200_H
+#define ATUM_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ATB_OK 0
+#define ATB_ERR_INVALID (-1)     /* bad argument / unsupported combination */
+#define ATB_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define ATB_ERR_NOMEM (-3)       /* device allocation failed */
+#define ATB_ERR_NONFINITE (-4)   /* NaN/Inf detected in a state */
+#define ATB_ERR_BUDGET (-5)      /* serving: request exceeds the HBM budget */
+#define ATB_ERR_TIMEOUT (-6)     /* bounded device wait expired */
+
+/* law: src/balancelaws/{advection,euler,euler_gravity,linear_euler_gravity,shallow_water}.jl */
+#define ATB_LAW_ADVECTION 0
+#define ATB_LAW_EULER 1
+#define ATB_LAW_EULER_GRAVITY 2
+#define ATB_LAW_LINEAR_EULER_GRAVITY 3
+#define ATB_LAW_SHALLOW_WATER 4
+/* numerical fluxes: src/numericalfluxes.jl:25-47 */
+#define ATB_FLUX_CENTRAL 0
+#define ATB_FLUX_RUSANOV 1
+#define ATB_FLUX_EC 2
+#define ATB_FLUX_KG 3
+#define ATB_FLUX_ROE 4
+#define ATB_FLUX_MATRIX 5
+/* boundarystate kinds (src/balancelaw.jl:21 and the reference's problem hooks) */
+#define ATB_BC_COPY 0
+#define ATB_BC_REFLECT 1
+#define ATB_BC_INFLOW_ZERO 2
+#define ATB_BC_DIRICHLET 3
+/* problem source! kinds */
+#define ATB_SRC_NONE 0
+#define ATB_SRC_CORIOLIS 1
+/* precision forms */
+#define ATB_PREC_FP64 0
+#define ATB_PREC_FP32FLUX 1
+/* solvers: src/odesolvers.jl */
+#define ATB_LSRK54 0
+#define ATB_LSRK144 1
+#define ATB_RLSRK54 2
+#define ATB_RLSRK144 3
+#define ATB_ARK23 4
+
+typedef struct atb_op atb_op;
+typedef struct atb_solver atb_solver;
+
+/* DGSEM(; law, grid, surface_numericalflux, volume_form, directions, auxstate)
+ * -- src/dgsem.jl:38-56.  The grid is Bennu's brickgrid (per-dimension vertex
+ * vectors, periodicity, Cartesian or stacked ordering); the 1-D LGL tables are
+ * the cell's nodes, weights and derivatives_1d(cell)[1] (row-major D[i][j] =
+ * l_j'(x_i)). */
+typedef struct {
+  int law, dim, N;
+  int K[3];
+  const double* vertices[3]; /* host, K[d]+1 each */
+  int periodic[3];
+  int stacked;               /* StackedOrdering{CartesianOrdering} */
+  int volume_form;           /* 0 WeakForm, 1 FluxDifferencingForm */
+  int volume_flux;           /* two-point flux of the flux-differencing form */
+  int fd_kernel;             /* 0 :per_dir, 1 :per_dir_symmetric, 2 :naive (same math) */
+  int surface_flux;
+  int directions;            /* bitmask, bit d = direction d+1 */
+  double gamma, grav;
+  double adv_u[3];
+  int sphere, pde_level_balance;
+  int bc_kind;
+  double bc_state[2][5];     /* Dirichlet: tag 1 -> [0], others -> [1] */
+  int source_kind;
+  double omega[3];
+  int sw_topography;         /* shallow-water bathymetry extension (aux = b, grad b) */
+  int naux;
+  int precision;             /* ATB_PREC_* */
+  const double* lgl_nodes;   /* host, Nq */
+  const double* lgl_weights; /* host, Nq */
+  const double* lgl_D;       /* host, Nq*Nq */
+} atb_op_desc;
+
+int atb_version(void);
+const char* atb_last_error(void);
+int atb_device_count(int* n);
+
+/* DGSEM construction (src/dgsem.jl:38-56); aux_host: naux*K*Np values in the
+ * field layout, evaluated on the host like auxiliary.(law, points(grid)). */
+int atb_op_create(const atb_op_desc* desc, const double* aux_host, atb_op** out);
+int atb_op_destroy(atb_op* op);
+int atb_op_dims(const atb_op* op, int* ns, int* K, int* Np);
+
+/* (dg::DGSEM)(dq, q, time; increment) -- src/dgsem.jl:59-98 */
+int atb_op_apply(atb_op* op, double* const* dq, const double* const* q, double time, int increment, void* stream);
+
+/* LSRK54/LSRK144/RLSRK54/RLSRK144/ARK23 constructors -- src/odesolvers.jl:59-67,138-146,284-309.
+ * rhs may be NULL for ARK23 (ARK23(nothing, linrhs, ...)); linrhs is NULL for the explicit kinds.
+ * For ARK23 the constructor probes linrhs and factors I - dt a_ii L once per distinct
+ * vertical column (src/bandedsystem.jl:1-15, src/odesolvers.jl:264-268). */
+int atb_solver_create(int kind, atb_op* rhs, atb_op* linrhs, double dt, double t0, int split_rhs, int paperversion,
+                      atb_solver** out);
+int atb_solver_destroy(atb_solver* s);
+/* dostep! repeated nsteps times -- src/odesolvers.jl:47-57,103-136,312-388 */
+int atb_solver_step(atb_solver* s, double* const* q, int nsteps, void* stream);
+/* solve!(q, timeend, solver; adjust_final) -- src/odesolvers.jl:9-26 */
+int atb_solve(atb_solver* s, double* const* q, double timeend, int adjust_final, int* steps_out, void* stream);
+int atb_solver_get(const atb_solver* s, double* time, double* dt, double* gamma);
+int atb_solver_set_dt(atb_solver* s, double dt);
+
+/* measures -- src/measures.jl:6-33 (p = 2 or INFINITY); results to host memory */
+int atb_weightednorm(atb_op* op, const double* const* q, double p, double* comp_host, double* total_host,
+                     void* stream);
+int atb_entropyintegral(atb_op* op, const double* const* q, double* out_host, void* stream);
+int atb_entropyproduct(atb_op* op, const double* const* p, const double* const* q, double* out_host, void* stream);
+/* NaN/Inf scan of a state: ATB_ERR_NONFINITE if any */
+int atb_check_finite(atb_op* op, const double* const* q, void* stream);
+
+/* device FP64 FMA throughput probe (measurement utility): runs a fixed FMA loop
+ * on every SM and returns the achieved FP64 TFLOP/s. */
+int atb_probe_fp64_peak(double* tflops, void* stream);
+
+/* Launch profiling (measurement utility, no reference counterpart).  When
+ * enabled, every kernel the library launches is bracketed by CUDA events on
+ * its own stream; atb_profile_read resolves them (synchronising) and returns
+ * launches and total milliseconds per kernel class:
+ *   0 tendency of an explicit / nonlinear operator, 1 tendency of an implicit
+ *   (linear) operator, 2 banded solve, 3 stage combinations, 4 reductions. */
+#define ATB_PROF_TEND 0
+#define ATB_PROF_TEND_LIN 1
+#define ATB_PROF_BAND 2
+#define ATB_PROF_COMBINE 3
+#define ATB_PROF_REDUCE 4
+int atb_profile_enable(int on);
+int atb_profile_reset(void);
+int atb_profile_read(int kclass, long* launches, double* total_ms);
+/* number of kernels launched by the library since load (all classes) */
+int atb_launch_count(long* n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ATUM_B200_H */

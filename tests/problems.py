@@ -123,7 +123,6 @@ def vortex_c1(N=3, K=8, steps=100, vflux="ec"):
     vf = A.FluxDifferencingForm(A.EntropyConservativeFlux() if vflux == "ec" else A.KennedyGruberFlux())
     dg = A.DGSEM(law=law, grid=grid, volume_form=vf, surface_numericalflux=A.RusanovFlux())
     dx = v[1] - v[0]
-    dt = 0.3 * dx / N
     g = law.gamma
 
     def vortex(x, t):
@@ -139,8 +138,14 @@ def vortex_c1(N=3, K=8, steps=100, vflux="ec"):
         return _pack(rho, *rhou, law.energy(rho, rhou, rho ** g))
 
     x = grid.points()
-    return Case("vortex_c1", dg, vortex(x, 0.0), dt, steps * dt, exact=lambda t: vortex(x, t),
-                extra={"steps": steps})
+    q0 = vortex(x, 0.0)
+    # CFL 0.3 in the reference tests' form dt = cfl * dx / N / speed, with the
+    # largest wave speed |u| + c of the initial state
+    rho, m, E = q0[0], q0[1:3], q0[3]
+    p = law.pressure(rho, list(m), E)
+    lam = float(np.max(np.sqrt(m[0] ** 2 + m[1] ** 2) / rho + np.sqrt(g * p / rho)))
+    dt = 0.3 * dx / N / lam
+    return Case("vortex_c1", dg, q0, dt, steps * dt, exact=lambda t: vortex(x, t), extra={"steps": steps})
 
 
 # ------------------------------------------------------ entropy conservation
