@@ -66,6 +66,7 @@ SIGNATURES = {
     "atb_profile_reset": [],
     "atb_profile_read": [C.c_int, C.POINTER(C.c_long), _DP],
     "atb_launch_count": [C.POINTER(C.c_long)],
+    "atb_lsrk54_step_noalloc": [_VP, PtrArr, C.c_double, C.c_int, _VP],
 }
 
 

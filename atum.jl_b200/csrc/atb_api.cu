@@ -1030,3 +1030,46 @@ extern "C" int atb_solver_set_dt(atb_solver* s, double dt) {
   s->dt = dt;
   return ATB_OK;
 }
+
+// ------------------------------------------- helpers for atb_noalloc.cu
+// LSRK(5,4) stages of `op` with caller-provided device scratch (dq and the
+// second state buffer): launches only, no allocation of any kind.
+int atb_detail_fail(int code, const char* msg) { return fail(code, "%s", msg); }
+
+int atb_detail_lsrk54_steps(atb_op* op, double* const* q, double* dqbuf, double* qbbuf, double dt, int nsteps,
+                            cudaStream_t st) {
+  static const double rka[5] = {0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
+                                -3550918686646.0 / 2091501179385.0, -1275806237668.0 / 842570457699.0};
+  static const double rkb[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+                                1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+                                2277821191437.0 / 14882151754819.0};
+  const int ns = op->ns;
+  const size_t n = op->stride();
+  double *dq[5], *cur[5], *oth[5];
+  for (int k = 0; k < 5; ++k) {
+    const int c = k < ns ? k : 0;
+    dq[k] = dqbuf + (size_t)c * n;
+    cur[k] = q[c];
+    oth[k] = qbbuf + (size_t)c * n;
+  }
+  bool in_user = true;
+  const int grid = (op->K + op->E - 1) / op->E;
+  for (int step = 0; step < nsteps; ++step)
+    for (int i = 0; i < 5; ++i) {
+      TendArgs A;
+      fill_args(op, A);
+      A.epi = EPI_LSRK;
+      A.a = rka[i];
+      A.bdt = rkb[i] * dt;
+      for (int k = 0; k < 5; ++k) { A.q[k] = cur[k]; A.out[k] = dq[k]; A.out2[k] = oth[k]; }
+      op->launch(A, grid, op->E * op->Np, op->smem, st);
+      const int rc = check_launch("tendency (no-alloc LSRK54)");
+      if (rc) return rc;
+      for (int k = 0; k < 5; ++k) std::swap(cur[k], oth[k]);
+      in_user = !in_user;
+    }
+  if (!in_user)
+    for (int s = 0; s < ns; ++s)
+      CK(cudaMemcpyAsync(q[s], cur[s], n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  return ATB_OK;
+}

@@ -153,6 +153,22 @@ int atb_profile_read(int kclass, long* launches, double* total_ms);
 /* number of kernels launched by the library since load (all classes) */
 int atb_launch_count(long* n);
 
+/* LSRK54 steps of an existing operator that allocate nothing.  No counterpart
+ * in the reference: it is for callers that cannot call cudaMalloc around a time
+ * step (an application whose device memory belongs to its own pool allocator,
+ * or a latency-critical loop that must not pay cudaMalloc/cudaFree's implicit
+ * synchronisation).  Same arithmetic as ATB_LSRK54 through atb_solver_step; the
+ * stage increment and the second state buffer live in a library-owned static
+ * device array of 2 * ATB_NOALLOC_MAX_DOFS doubles (8 MiB, held by every GPU that
+ * loads the library until exit).  States with more than ATB_NOALLOC_MAX_DOFS
+ * DOFs (ns*K*Np) are rejected with ATB_ERR_INVALID.  The first call on a device
+ * looks up the array's device address for that device (cudaGetSymbolAddress);
+ * make that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU race on it and must be serialised by the caller;
+ * the increment is cleared at the start of each call. */
+#define ATB_NOALLOC_MAX_DOFS 524288
+int atb_lsrk54_step_noalloc(atb_op* op, double* const* q, double dt, int nsteps, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
