@@ -26,6 +26,11 @@ template <> tend_launch_fn pick_launcher<LAW_EULER>(int, int);
 template <> tend_launch_fn pick_launcher<LAW_EG>(int, int);
 template <> tend_launch_fn pick_launcher<LAW_LEG>(int, int);
 template <> tend_launch_fn pick_launcher<LAW_SW>(int, int);
+template <> tend_launch_fn pick_launcher_nq<LAW_ADV>(int, int, int);
+template <> tend_launch_fn pick_launcher_nq<LAW_EULER>(int, int, int);
+template <> tend_launch_fn pick_launcher_nq<LAW_EG>(int, int, int);
+template <> tend_launch_fn pick_launcher_nq<LAW_LEG>(int, int, int);
+template <> tend_launch_fn pick_launcher_nq<LAW_SW>(int, int, int);
 template <> red_launch_fn pick_reducer<LAW_ADV>(int);
 template <> red_launch_fn pick_reducer<LAW_EULER>(int);
 template <> red_launch_fn pick_reducer<LAW_EG>(int);
@@ -290,12 +295,15 @@ extern "C" int atb_op_create(const atb_op_desc* d, const double* aux_host, atb_o
   }
   tend_launch_fn fn = nullptr;
   red_launch_fn rf = nullptr;
+  // a compile-time node-count specialisation when one exists, else the
+  // runtime-Nq kernel
+  const int nq = d->N + 1;
   switch (d->law) {
-    case LAW_ADV: fn = pick_launcher<LAW_ADV>(d->dim, vk); rf = pick_reducer<LAW_ADV>(d->dim); break;
-    case LAW_EULER: fn = pick_launcher<LAW_EULER>(d->dim, vk); rf = pick_reducer<LAW_EULER>(d->dim); break;
-    case LAW_EG: fn = pick_launcher<LAW_EG>(d->dim, vk); rf = pick_reducer<LAW_EG>(d->dim); break;
-    case LAW_LEG: fn = pick_launcher<LAW_LEG>(d->dim, vk); rf = pick_reducer<LAW_LEG>(d->dim); break;
-    case LAW_SW: fn = pick_launcher<LAW_SW>(d->dim, vk); rf = pick_reducer<LAW_SW>(d->dim); break;
+    case LAW_ADV: fn = pick_launcher_nq<LAW_ADV>(d->dim, vk, nq); if (!fn) fn = pick_launcher<LAW_ADV>(d->dim, vk); rf = pick_reducer<LAW_ADV>(d->dim); break;
+    case LAW_EULER: fn = pick_launcher_nq<LAW_EULER>(d->dim, vk, nq); if (!fn) fn = pick_launcher<LAW_EULER>(d->dim, vk); rf = pick_reducer<LAW_EULER>(d->dim); break;
+    case LAW_EG: fn = pick_launcher_nq<LAW_EG>(d->dim, vk, nq); if (!fn) fn = pick_launcher<LAW_EG>(d->dim, vk); rf = pick_reducer<LAW_EG>(d->dim); break;
+    case LAW_LEG: fn = pick_launcher_nq<LAW_LEG>(d->dim, vk, nq); if (!fn) fn = pick_launcher<LAW_LEG>(d->dim, vk); rf = pick_reducer<LAW_LEG>(d->dim); break;
+    case LAW_SW: fn = pick_launcher_nq<LAW_SW>(d->dim, vk, nq); if (!fn) fn = pick_launcher<LAW_SW>(d->dim, vk); rf = pick_reducer<LAW_SW>(d->dim); break;
   }
   if (!fn) return fail(ATB_ERR_INVALID, "unsupported (law %d, volume flux %d) combination", d->law, d->volume_flux);
   const int sf = d->surface_flux;
@@ -408,7 +416,7 @@ extern "C" int atb_op_create(const atb_op_desc* d, const double* aux_host, atb_o
   if (d->law == LAW_LEG) nu = dim + 3;
   if (d->law == LAW_SW && d->sw_topography) nu = (vk == VK_WEAK) ? dim + 1 : 1;
   op->naux_used = std::min(nu, op->naux);
-  const int npre = npre_of(d->law, dim, vk), npv = npv_of(d->law, dim, vk);
+  const int npre = npre_of(d->law, dim, vk), npv = npv_stride_of(d->law, dim, vk);
   op->E = std::max(1, 256 / Np);
   while (op->E > 1 &&
          tend_smem_bytes(op->ns, npre, op->naux_used, dim, Nq, Np, op->Nfp, op->E, npv) > 100 * 1024)

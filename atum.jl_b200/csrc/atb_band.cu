@@ -44,7 +44,7 @@ __global__ void __launch_bounds__(LPB) band_solve_shared_kernel(const BandSolve 
   constexpr int WP = 2 * BW1;  // padded row stride (2*bw + 1 entries + 1 pad)
   constexpr int BLK = BW1 * WP;
   extern __shared__ __align__(16) double sband[];
-  double* sbuf[2] = {sband, sband + BLK};
+  auto sbuf = [&](int b) { return sband + b * BLK; };
   const LineMap& M = B.M;
   const int line = blockIdx.x * LPB + threadIdx.x;
   const bool act = line < M.nlines;
@@ -55,9 +55,9 @@ __global__ void __launch_bounds__(LPB) band_solve_shared_kernel(const BandSolve 
   const int npairs = B.npairs;
 
   // ------------------------------------------------------------ forward
-  stage_block<BLK, LPB>(sbuf[0], band);
+  stage_block<BLK, LPB>(sbuf(0), band);
   cp_async_commit();
-  if (KV > 1) stage_block<BLK, LPB>(sbuf[1], band + BLK);
+  if (KV > 1) stage_block<BLK, LPB>(sbuf(1), band + BLK);
   cp_async_commit();
   double prev[BW1], cur[BW1];
 #pragma unroll
@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(LPB) band_solve_shared_kernel(const BandSolve 
   for (int ev = 0; ev < KV; ++ev) {
     cp_async_wait1();
     __syncthreads();
-    const double* Lb = sbuf[ev & 1];
+    const double* Lb = sbuf(ev & 1);
     if (act) {
       const size_t eoff = (size_t)(e0 + ev * M.estep) * Np + hn;
 #pragma unroll
@@ -73,7 +73,9 @@ __global__ void __launch_bounds__(LPB) band_solve_shared_kernel(const BandSolve 
         const int s = i % NS, kv = i / NS;
         const size_t g = eoff + (size_t)nh * kv;
         double acc = B.q[s][g];
-        for (int k = 0; k < npairs; ++k) acc = acc + B.dt * (B.a[k] * B.ex[k][s][g] + B.b[k] * B.im[k][s][g]);
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+          if (k < npairs) acc = acc + B.dt * (B.a[k] * B.ex[k][s][g] + B.b[k] * B.im[k][s][g]);
         const double* row = Lb + i * WP;
 #pragma unroll
         for (int j = i + 1; j < BW1; ++j) acc = acc - row[j - i - 1] * prev[j];
@@ -86,16 +88,16 @@ __global__ void __launch_bounds__(LPB) band_solve_shared_kernel(const BandSolve 
       for (int j = 0; j < BW1; ++j) prev[j] = cur[j];
     }
     __syncthreads();
-    if (ev + 2 < KV) stage_block<BLK, LPB>(sbuf[ev & 1], band + (size_t)(ev + 2) * BLK);
+    if (ev + 2 < KV) stage_block<BLK, LPB>(sbuf(ev & 1), band + (size_t)(ev + 2) * BLK);
     cp_async_commit();
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncthreads();
 
   // ----------------------------------------------------------- backward
-  stage_block<BLK, LPB>(sbuf[0], band + (size_t)(KV - 1) * BLK);
+  stage_block<BLK, LPB>(sbuf(0), band + (size_t)(KV - 1) * BLK);
   cp_async_commit();
-  if (KV > 1) stage_block<BLK, LPB>(sbuf[1], band + (size_t)(KV - 2) * BLK);
+  if (KV > 1) stage_block<BLK, LPB>(sbuf(1), band + (size_t)(KV - 2) * BLK);
   cp_async_commit();
   double nxt[BW1];
 #pragma unroll
@@ -104,7 +106,7 @@ __global__ void __launch_bounds__(LPB) band_solve_shared_kernel(const BandSolve 
     const int ev = KV - 1 - t;
     cp_async_wait1();
     __syncthreads();
-    const double* Ub = sbuf[t & 1];
+    const double* Ub = sbuf(t & 1);
     if (act) {
       const size_t eoff = (size_t)(e0 + ev * M.estep) * Np + hn;
 #pragma unroll
@@ -125,7 +127,7 @@ __global__ void __launch_bounds__(LPB) band_solve_shared_kernel(const BandSolve 
       for (int j = 0; j < BW1; ++j) nxt[j] = cur[j];
     }
     __syncthreads();
-    if (ev - 2 >= 0) stage_block<BLK, LPB>(sbuf[t & 1], band + (size_t)(ev - 2) * BLK);
+    if (ev - 2 >= 0) stage_block<BLK, LPB>(sbuf(t & 1), band + (size_t)(ev - 2) * BLK);
     cp_async_commit();
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -181,96 +183,137 @@ __global__ void block_prep_kernel(const double* band, int KV, int BW1, double* b
   }
 }
 
+// One thread per (node kv of the element column, line l): it owns the NS rows
+// kv*NS .. kv*NS+NS-1 of every element block of its line.  Per element it
+// reads the line's right-hand-side / previous-solution vectors (2*BW1 values,
+// shared by its NS rows) and its NS rows of the two matrices (warp-uniform
+// addresses -> broadcasts, two doubles per load), and issues NS*2*BW1 FMAs.
+// Warps hold 32 lines at the same kv, so the global accesses of a state
+// component are consecutive addresses.
 template <int NQ, int NS, int LPB>
-__global__ void __launch_bounds__(NQ * NS * LPB) band_solve_block_kernel(const BandSolve B, const double* blk) {
+__global__ void __launch_bounds__(NQ * LPB) band_solve_block_kernel(const BandSolve B, const double* blk) {
   constexpr int BW1 = NQ * NS;
   constexpr int MAT = BW1 * BW1;
   extern __shared__ __align__(16) double sm[];
-  double* smat[2] = {sm, sm + 2 * MAT};          // [Li|G] or [Ui|H], double-buffered
-  double* ys = sm + 4 * MAT;                     // [2][BW1][LPB]
-  double* bs = ys + 2 * BW1 * LPB;               // [BW1][LPB]
+  // smat(b): [Li|G] or [Ui|H], double-buffered (arithmetic, not a pointer
+  // array: a runtime-indexed local array would live in local memory)
+  auto smat = [&](int b) { return sm + b * 2 * MAT; };
+  double* ys = sm + 4 * MAT;             // [2][BW1][LPB]
+  double* bs = ys + 2 * BW1 * LPB;       // [BW1][LPB]
   const LineMap& M = B.M;
-  const int l = threadIdx.x % LPB, r = threadIdx.x / LPB;
+  const int l = threadIdx.x % LPB, kv = threadIdx.x / LPB;
   const int line = blockIdx.x * LPB + l;
   const bool act = line < M.nlines;
   const int KV = M.KV, nh = M.nh, Np = M.Np;
   const int hn = act ? line % nh : 0;
   const int e0 = act ? M.e0[line] : 0;
-  const int s = r % NS, kv = r / NS;
-  const int nthr = BW1 * LPB;
+  const int nthr = NQ * LPB;
   auto stage = [&](double* dst, const double* src) {
     for (int c = threadIdx.x; c < MAT; c += nthr) cp_async16(dst + 2 * c, src + 2 * c);  // 2*MAT doubles
   };
-  // ------------------------------------------------------------ forward
-  stage(smat[0], blk);
-  cp_async_commit();
-  if (KV > 1) stage(smat[1], blk + (size_t)4 * MAT);
-  cp_async_commit();
-  ys[r * LPB + l] = 0.0;  // y_{-1} = 0 (buffer 1 is "previous" for ev = 0)
-  ys[BW1 * LPB + r * LPB + l] = 0.0;
-  for (int ev = 0; ev < KV; ++ev) {
-    const size_t g = (size_t)(e0 + ev * M.estep) * Np + hn + (size_t)nh * kv;
-    double b = 0.0;
-    if (act) {
-      b = B.q[s][g];
-      for (int k = 0; k < B.npairs; ++k) b = b + B.dt * (B.a[k] * B.ex[k][s][g] + B.b[k] * B.im[k][s][g]);
-    }
-    bs[r * LPB + l] = b;
-    cp_async_wait1();
-    __syncthreads();
-    const double* Li = smat[ev & 1] + r * BW1;
-    const double* G = Li + MAT;
-    const double* yprev = ys + ((ev + 1) & 1) * BW1 * LPB;
-    double z0 = 0.0, z1 = 0.0, w0 = 0.0, w1 = 0.0;
+  auto gidx = [&](int ev) { return (size_t)(e0 + ev * M.estep) * Np + hn + (size_t)nh * kv; };
+  // y_e = A_e v_e - C_e w_e-1 for this thread's NS rows (A, C row-major BW1 x BW1)
+  auto block_rows = [&](const double* Am, const double* Cm, const double* v, const double* w, double* out) {
 #pragma unroll
-    for (int k = 0; k < BW1; k += 2) {
-      z0 += Li[k] * bs[k * LPB + l];
-      w0 += G[k] * yprev[k * LPB + l];
-      if (k + 1 < BW1) {
-        z1 += Li[k + 1] * bs[(k + 1) * LPB + l];
-        w1 += G[k + 1] * yprev[(k + 1) * LPB + l];
+    for (int s = 0; s < NS; ++s) out[s] = 0.0;
+    double acc2[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) acc2[s] = 0.0;
+#pragma unroll
+    for (int k = 0; k < BW1; ++k) {
+      const double vk = v[k * LPB + l], wk = w[k * LPB + l];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const int row = kv * NS + s;
+        out[s] += Am[row * BW1 + k] * vk;
+        acc2[s] += Cm[row * BW1 + k] * wk;
       }
     }
-    const double y = (z0 + z1) - (w0 + w1);
-    ys[(ev & 1) * BW1 * LPB + r * LPB + l] = y;
-    if (act) B.out[s][g] = y;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) out[s] -= acc2[s];
+  };
+  // ------------------------------------------------------------ forward
+  stage(smat(0), blk);
+  cp_async_commit();
+  if (KV > 1) stage(smat(1), blk + (size_t)4 * MAT);
+  cp_async_commit();
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    ys[(kv * NS + s) * LPB + l] = 0.0;  // y_{-1} = 0
+    ys[BW1 * LPB + (kv * NS + s) * LPB + l] = 0.0;
+  }
+  double bnext[NS];
+  auto rhs = [&](int ev, double* b) {
+    const size_t g = gidx(ev);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      double v = 0.0;
+      if (act) {
+        v = B.q[s][g];
+        // static pair index: the kernel-parameter pointer tables stay in the
+        // constant bank instead of being copied to local memory
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+          if (k < B.npairs) v = v + B.dt * (B.a[k] * B.ex[k][s][g] + B.b[k] * B.im[k][s][g]);
+      }
+      b[s] = v;
+    }
+  };
+  rhs(0, bnext);
+  for (int ev = 0; ev < KV; ++ev) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) bs[(kv * NS + s) * LPB + l] = bnext[s];
+    if (ev + 1 < KV) rhs(ev + 1, bnext);
+    cp_async_wait1();
     __syncthreads();
-    if (ev + 2 < KV) stage(smat[ev & 1], blk + (size_t)(ev + 2) * 4 * MAT);
+    double y[NS];
+    block_rows(smat(ev & 1), smat(ev & 1) + MAT, bs, ys + ((ev + 1) & 1) * BW1 * LPB, y);
+    const size_t g = gidx(ev);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      ys[(ev & 1) * BW1 * LPB + (kv * NS + s) * LPB + l] = y[s];
+      if (act) B.out[s][g] = y[s];
+    }
+    __syncthreads();
+    if (ev + 2 < KV) stage(smat(ev & 1), blk + (size_t)(ev + 2) * 4 * MAT);
     cp_async_commit();
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncthreads();
   // ----------------------------------------------------------- backward
-  stage(smat[0], blk + (size_t)(KV - 1) * 4 * MAT + 2 * MAT);
+  stage(smat(0), blk + (size_t)(KV - 1) * 4 * MAT + 2 * MAT);
   cp_async_commit();
-  if (KV > 1) stage(smat[1], blk + (size_t)(KV - 2) * 4 * MAT + 2 * MAT);
+  if (KV > 1) stage(smat(1), blk + (size_t)(KV - 2) * 4 * MAT + 2 * MAT);
   cp_async_commit();
-  ys[r * LPB + l] = 0.0;
-  ys[BW1 * LPB + r * LPB + l] = 0.0;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    ys[(kv * NS + s) * LPB + l] = 0.0;
+    ys[BW1 * LPB + (kv * NS + s) * LPB + l] = 0.0;
+  }
+  double ynext[NS];
+  auto yload = [&](int ev, double* yv) {
+    const size_t g = gidx(ev);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) yv[s] = act ? B.out[s][g] : 0.0;
+  };
+  yload(KV - 1, ynext);
   for (int t = 0; t < KV; ++t) {
     const int ev = KV - 1 - t;
-    const size_t g = (size_t)(e0 + ev * M.estep) * Np + hn + (size_t)nh * kv;
-    bs[r * LPB + l] = act ? B.out[s][g] : 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) bs[(kv * NS + s) * LPB + l] = ynext[s];
+    if (ev > 0) yload(ev - 1, ynext);
     cp_async_wait1();
     __syncthreads();
-    const double* Ui = smat[t & 1] + r * BW1;
-    const double* H = Ui + MAT;
-    const double* xnext = ys + ((t + 1) & 1) * BW1 * LPB;
-    double z0 = 0.0, z1 = 0.0, w0 = 0.0, w1 = 0.0;
+    double x[NS];
+    block_rows(smat(t & 1), smat(t & 1) + MAT, bs, ys + ((t + 1) & 1) * BW1 * LPB, x);
+    const size_t g = gidx(ev);
 #pragma unroll
-    for (int k = 0; k < BW1; k += 2) {
-      z0 += Ui[k] * bs[k * LPB + l];
-      w0 += H[k] * xnext[k * LPB + l];
-      if (k + 1 < BW1) {
-        z1 += Ui[k + 1] * bs[(k + 1) * LPB + l];
-        w1 += H[k + 1] * xnext[(k + 1) * LPB + l];
-      }
+    for (int s = 0; s < NS; ++s) {
+      ys[(t & 1) * BW1 * LPB + (kv * NS + s) * LPB + l] = x[s];
+      if (act) B.out[s][g] = x[s];
     }
-    const double x = (z0 + z1) - (w0 + w1);
-    ys[(t & 1) * BW1 * LPB + r * LPB + l] = x;
-    __syncthreads();  // every row has read its y before any row overwrites it
-    if (act) B.out[s][g] = x;
-    if (ev - 2 >= 0) stage(smat[t & 1], blk + (size_t)(ev - 2) * 4 * MAT + 2 * MAT);
+    __syncthreads();
+    if (ev - 2 >= 0) stage(smat(t & 1), blk + (size_t)(ev - 2) * 4 * MAT + 2 * MAT);
     cp_async_commit();
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -306,13 +349,13 @@ template <int NS> solve_fn pick_nq(int nq) {
 
 template <int NQ, int NS> void block_launch(const BandSolve& B, cudaStream_t st) {
   constexpr int BW1 = NQ * NS;
-  constexpr int LPB = (BW1 >= 20) ? 8 : 32;
+  constexpr int LPB = 32;
   constexpr size_t smem = sizeof(double) * (4 * BW1 * BW1 + 3 * BW1 * LPB);
   static bool configured = false;
   if (!configured && smem > 48 * 1024)
     cudaFuncSetAttribute(band_solve_block_kernel<NQ, NS, LPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   configured = true;
-  band_solve_block_kernel<NQ, NS, LPB><<<(B.M.nlines + LPB - 1) / LPB, BW1 * LPB, smem, st>>>(B, B.blk);
+  band_solve_block_kernel<NQ, NS, LPB><<<(B.M.nlines + LPB - 1) / LPB, NQ * LPB, smem, st>>>(B, B.blk);
 }
 
 template <int NS> solve_fn pick_block(int nq) {

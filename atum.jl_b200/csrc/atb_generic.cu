@@ -6,12 +6,19 @@
 namespace atb {
 
 // ------------------------------------------------------------ elementwise
+// Loops run to their compile-time maxima with runtime guards so that every
+// pointer-table index is static (a runtime index would copy the kernel
+// parameters to local memory).
 __global__ void lincomb_kernel(const LinComb C) {
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < C.n; i += stride) {
-    for (int s = 0; s < C.ns; ++s) {
+#pragma unroll
+    for (int s = 0; s < 5; ++s) {
+      if (s >= C.ns) break;
       double acc = C.base[s][i];
-      for (int k = 0; k < C.npairs; ++k) acc = acc + C.dt * (C.a[k] * C.X[k][s][i] + C.b[k] * C.Y[k][s][i]);
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+        if (k < C.npairs) acc = acc + C.dt * (C.a[k] * C.X[k][s][i] + C.b[k] * C.Y[k][s][i]);
       C.out[s][i] = acc;
     }
   }
@@ -29,8 +36,11 @@ void launch_lincomb(const LinComb& C, cudaStream_t st) {
 
 __global__ void axpy_kernel(const Axpy A) {
   const size_t stride = (size_t)gridDim.x * blockDim.x;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += stride)
-    for (int s = 0; s < A.ns; ++s) A.out[s][i] = A.x[s][i] + A.c * A.y[s][i];
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += stride) {
+#pragma unroll
+    for (int s = 0; s < 5; ++s)
+      if (s < A.ns) A.out[s][i] = A.x[s][i] + A.c * A.y[s][i];
+  }
 }
 
 void launch_axpy(const Axpy& A, cudaStream_t st) { axpy_kernel<<<grid_for(A.n, 256), 256, 0, st>>>(A); }

@@ -1,21 +1,21 @@
-// Tendency-kernel instantiations for LAW_EULER (one file per law so the
-// instantiations compile in parallel).
+// Tendency-kernel instantiations for LAW_EULER with a runtime node count
+// (one file per law so the instantiations compile in parallel).
 #include "atb_tendency.cuh"
 #include "atb_reduce.cuh"
 namespace atb {
 template <> tend_launch_fn pick_launcher<LAW_EULER>(int dim, int vk) {
-  if (dim == 1 && vk == VK_WEAK) return tend_launch<LAW_EULER, 1, VK_WEAK>;
-  if (dim == 1 && vk == VK_CENTRAL) return tend_launch<LAW_EULER, 1, VK_CENTRAL>;
-  if (dim == 1 && vk == VK_EC) return tend_launch<LAW_EULER, 1, VK_EC>;
-  if (dim == 1 && vk == VK_KG) return tend_launch<LAW_EULER, 1, VK_KG>;
-  if (dim == 2 && vk == VK_WEAK) return tend_launch<LAW_EULER, 2, VK_WEAK>;
-  if (dim == 2 && vk == VK_CENTRAL) return tend_launch<LAW_EULER, 2, VK_CENTRAL>;
-  if (dim == 2 && vk == VK_EC) return tend_launch<LAW_EULER, 2, VK_EC>;
-  if (dim == 2 && vk == VK_KG) return tend_launch<LAW_EULER, 2, VK_KG>;
-  if (dim == 3 && vk == VK_WEAK) return tend_launch<LAW_EULER, 3, VK_WEAK>;
-  if (dim == 3 && vk == VK_CENTRAL) return tend_launch<LAW_EULER, 3, VK_CENTRAL>;
-  if (dim == 3 && vk == VK_EC) return tend_launch<LAW_EULER, 3, VK_EC>;
-  if (dim == 3 && vk == VK_KG) return tend_launch<LAW_EULER, 3, VK_KG>;
+  if (dim == 1 && vk == VK_WEAK) return tend_launch<LAW_EULER, 1, VK_WEAK, 0>;
+  if (dim == 1 && vk == VK_CENTRAL) return tend_launch<LAW_EULER, 1, VK_CENTRAL, 0>;
+  if (dim == 1 && vk == VK_EC) return tend_launch<LAW_EULER, 1, VK_EC, 0>;
+  if (dim == 1 && vk == VK_KG) return tend_launch<LAW_EULER, 1, VK_KG, 0>;
+  if (dim == 2 && vk == VK_WEAK) return tend_launch<LAW_EULER, 2, VK_WEAK, 0>;
+  if (dim == 2 && vk == VK_CENTRAL) return tend_launch<LAW_EULER, 2, VK_CENTRAL, 0>;
+  if (dim == 2 && vk == VK_EC) return tend_launch<LAW_EULER, 2, VK_EC, 0>;
+  if (dim == 2 && vk == VK_KG) return tend_launch<LAW_EULER, 2, VK_KG, 0>;
+  if (dim == 3 && vk == VK_WEAK) return tend_launch<LAW_EULER, 3, VK_WEAK, 0>;
+  if (dim == 3 && vk == VK_CENTRAL) return tend_launch<LAW_EULER, 3, VK_CENTRAL, 0>;
+  if (dim == 3 && vk == VK_EC) return tend_launch<LAW_EULER, 3, VK_EC, 0>;
+  if (dim == 3 && vk == VK_KG) return tend_launch<LAW_EULER, 3, VK_KG, 0>;
   return nullptr;
 }
 template <> red_launch_fn pick_reducer<LAW_EULER>(int dim) {

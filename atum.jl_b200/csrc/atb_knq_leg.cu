@@ -1,0 +1,27 @@
+// Compile-time node-count specialisations of the tendency kernel (hot
+// configurations; the runtime-Nq kernel covers everything else).
+#include "atb_tendency.cuh"
+namespace atb {
+tend_launch_fn pick_nq_leg_3_vk_weak(int nq) {
+  switch (nq) {
+    case 3: return tend_launch<LAW_LEG, 3, VK_WEAK, 3>;
+    case 4: return tend_launch<LAW_LEG, 3, VK_WEAK, 4>;
+    case 5: return tend_launch<LAW_LEG, 3, VK_WEAK, 5>;
+    case 6: return tend_launch<LAW_LEG, 3, VK_WEAK, 6>;
+    case 7: return tend_launch<LAW_LEG, 3, VK_WEAK, 7>;
+    case 8: return tend_launch<LAW_LEG, 3, VK_WEAK, 8>;
+  }
+  return nullptr;
+}
+tend_launch_fn pick_nq_leg_2_vk_weak(int nq) {
+  switch (nq) {
+    case 3: return tend_launch<LAW_LEG, 2, VK_WEAK, 3>;
+    case 4: return tend_launch<LAW_LEG, 2, VK_WEAK, 4>;
+    case 5: return tend_launch<LAW_LEG, 2, VK_WEAK, 5>;
+    case 6: return tend_launch<LAW_LEG, 2, VK_WEAK, 6>;
+    case 7: return tend_launch<LAW_LEG, 2, VK_WEAK, 7>;
+    case 8: return tend_launch<LAW_LEG, 2, VK_WEAK, 8>;
+  }
+  return nullptr;
+}
+}  // namespace atb

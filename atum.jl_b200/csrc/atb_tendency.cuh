@@ -55,9 +55,14 @@ struct TendArgs {
   double* out2[5];
 };
 
+// Per-node values staged for the volume term:
+//   EC (Euler / Euler-gravity): u (DIM), b = rho/2p, |u|^2, p/rho
+//   KG: u (DIM), p, e = rho e / rho
+//   EC (shallow water): u (DIM), theta
+//   weak / central forms: the DIM physical flux rows (DIM * NS)
 template <int LAW, int DIM, int VK> struct NPre {
   static constexpr int NS = NSt<LAW, DIM>::v;
-  static constexpr int v = (VK == VK_EC || VK == VK_KG) ? ((LAW == LAW_SW) ? DIM + 1 : DIM + 5) : DIM * NS;
+  static constexpr int v = (VK == VK_EC) ? ((LAW == LAW_SW) ? DIM + 1 : DIM + 3) : (VK == VK_KG) ? DIM + 2 : DIM * NS;
 };
 // upper bound of the aux components a kernel stages (compile time, so the
 // per-thread aux arrays stay in registers)
@@ -65,30 +70,164 @@ template <int LAW, int DIM> struct NAuxMax {
   static constexpr int v = (LAW == LAW_EG || LAW == LAW_LEG) ? DIM + 3 : (LAW == LAW_SW) ? DIM + 1 : 1;
 };
 // values stored per node pair: row d of the symmetric two-point flux, plus
-// b_avg * rho_log for the Euler-gravity EC fluctuation
+// b_avg * rho_log for the Euler-gravity EC fluctuation; the stride is odd so
+// that consecutive pairs fall in different shared-memory banks
 template <int LAW, int DIM, int VK> struct NPairVals {
   static constexpr int v = NSt<LAW, DIM>::v + ((LAW == LAW_EG && VK == VK_EC) ? 1 : 0);
+  static constexpr int stride = v | 1;
 };
 
-inline size_t tend_smem_bytes(int ns, int npre, int naux, int dim, int Nq, int Np, int Nfp, int E, int npv) {
+inline size_t tend_smem_bytes(int ns, int npre, int naux, int dim, int Nq, int Np, int Nfp, int E, int npvs) {
   const int npl = Nq * (Nq - 1) / 2;
   size_t per = (size_t)(ns + naux + npre) * Np + (size_t)2 * dim * Nfp * ns;
-  if (npv > 0) per += (size_t)Nfp * npl * npv;
+  if (npvs > 0) per += (size_t)Nfp * npl * npvs;
   return sizeof(double) * (2 * (size_t)Nq * Nq + 2 + per * E) + 64 * sizeof(int);
+}
+
+__host__ __device__ constexpr int ipow(int b, int e) { return e == 0 ? 1 : b * ipow(b, e - 1); }
+
+// volume-term two-point fluxes on the staged per-node layouts (row d)
+//
+// EC flux: when both logarithmic means are on their series branch
+// (u = ((a-b)/(a+b))^2 < 1e-4 for rho and for b, the common case between
+// neighbouring nodes of a resolved flow) every division of the flux shares
+// ONE reciprocal, 1/((r1+r2)^2 (b1+b2)^2):
+//   rho_log = (r1+r2)/2 * G(u_rho),  b_log = (b1+b2)/2 * G(u_b),
+//   rho_avg/(2 b_avg) = (r1+r2)/2 / (b1+b2),
+//   1/(2 (gamma-1) b_log) = F(u_b) / ((gamma-1) (b1+b2)),
+// with F(u) = 1 + u/3 + u^2/5 + u^3/7 + u^4/9 (the reference's series) and
+// G = 1/F = 1 - u/3 - 4u^2/45 - 44u^3/945 - 428u^4/14175 (truncation below
+// 3e-22 relative for u < 1e-4).  Otherwise the general form below is used.
+template <class T> __device__ __forceinline__ T series_F(T u) {
+  return T(1) + u * (T(1) / T(3) + u * (T(1) / T(5) + u * (T(1) / T(7) + u * (T(1) / T(9)))));
+}
+template <class T> __device__ __forceinline__ T series_G(T u) {
+  return T(1) - u * (T(1) / T(3) + u * (T(4) / T(45) + u * (T(44) / T(945) + u * (T(428) / T(14175)))));
+}
+
+template <int LAW, int DIM, class T>
+__device__ __forceinline__ void ec_vol(T gamma, T igm1, int d, T r1, const T* P1, T Phi1, T r2, const T* P2, T Phi2,
+                                       T* f, T* xtra) {
+  const T rho_avg = (r1 + r2) / T(2);
+  T ua[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) ua[c] = (P1[c] + P2[c]) / T(2);
+  const T b1 = P1[DIM], b2 = P2[DIM];
+  const T b_avg = (b1 + b2) / T(2);
+  const T u2_avg = (P1[DIM + 1] + P2[DIM + 1]) / T(2);
+  const T rs = r1 + r2, rd = r1 - r2, bs = b1 + b2, bd = b1 - b2;
+  const T rs2 = rs * rs, bs2 = bs * bs, rd2 = rd * rd, bd2 = bd * bd;
+  T rho_log, pc, cterm;
+  if (rd2 < T(1e-4) * rs2 && bd2 < T(1e-4) * bs2) {
+    const T inv = T(1) / (rs2 * bs2);
+    const T ur = rd2 * bs2 * inv, ub = bd2 * rs2 * inv;
+    const T inv_bs = bs * rs2 * inv;  // 1 / (b1 + b2)
+    rho_log = rho_avg * series_G(ur);
+    pc = rho_avg * inv_bs;
+    cterm = series_F(ub) * inv_bs * igm1;
+  } else {
+    rho_log = logavg_fast(r1, r2);
+    const T b_log = logavg_fast(b1, b2);
+    const T rinv = T(1) / (b_avg * b_log);  // shared by rho_avg/(2 b_avg) and 1/(2(gamma-1) b_log)
+    pc = rho_avg * b_log * rinv / T(2);
+    cterm = b_avg * rinv * igm1 / T(2);
+  }
+  (void)gamma;
+  const T ud = ua[d];
+  const T frd = ud * rho_log;
+  f[0] = frd;
+  T mu = T(0);
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    T m = ud * (ua[c] * rho_log);
+    if (c == d) m = m + pc;
+    f[1 + c] = m;
+    mu = (c == 0) ? m * ua[c] : mu + m * ua[c];
+  }
+  T c1 = cterm - u2_avg / T(2);
+  if (LAW == LAW_EG) c1 = c1 + (Phi1 + Phi2) / T(2);
+  f[DIM + 1] = c1 * frd + mu;
+  *xtra = b_avg * rho_log;
+}
+
+template <int DIM, class T>
+__device__ __forceinline__ void kg_vol(int d, T r1, const T* P1, T r2, const T* P2, T* f) {
+  const T rho_avg = (r1 + r2) / T(2);
+  const T ud = (P1[d] + P2[d]) / T(2);
+  const T p_avg = (P1[DIM] + P2[DIM]) / T(2);
+  const T e_avg = (P1[DIM + 1] + P2[DIM + 1]) / T(2);
+  const T frd = ud * rho_avg;
+  f[0] = frd;
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    T m = ud * (((P1[c] + P2[c]) / T(2)) * rho_avg);
+    if (c == d) m = m + p_avg;
+    f[1 + c] = m;
+  }
+  f[DIM + 1] = ud * (rho_avg * e_avg + p_avg);
 }
 
 // pair index of nodes a < b on a line of Nq nodes
 __device__ __forceinline__ int pair_index(int a, int b, int Nq) { return a * Nq - a * (a + 1) / 2 + (b - a - 1); }
 
-template <int LAW, int DIM, int VK>
+// one face-node task (face t / Nfp of direction D_, node t % Nfp): gather
+// the neighbour trace (or the boundary state), evaluate the numerical flux and
+// store it lifted into the face's shared-memory slot
+template <int LAW, int DIM, int NAM, int D_>
+__device__ __forceinline__ void face_task(const TendArgs& A, const LawP& L, int Nq, int Np, int Nfp, int e, int t,
+                                          const double* sq, const double* sa, double* ss, double gid,
+                                          double lift_end) {
+  constexpr int NS = NSt<LAW, DIM>::v;
+  const int naux = A.naux;
+  const int face = t / Nfp, j = t - face * Nfp;
+  const int side = face & 1;
+  if (!((A.dirs >> D_) & 1)) return;
+  const int t0 = j % Nq, t1 = j / Nq;
+  const int fix = side ? Nq - 1 : 0;
+  const int nm = (D_ == 0) ? fix + Nq * (t0 + Nq * t1) : (D_ == 1) ? t0 + Nq * (fix + Nq * t1) : t0 + Nq * (t1 + Nq * fix);
+  double qm[NS], qp[NS], am[NAM], ap[NAM];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) qm[s] = sq[s * Np + nm];
+#pragma unroll
+  for (int k = 0; k < NAM; ++k) am[k] = (k < naux) ? sa[k * Np + nm] : 0.0;
+  const int nb = __ldg(A.nbr + 6 * e + face);
+  const double sgn = side ? 1.0 : -1.0;
+  if (nb >= 0) {
+    const int stride_d = (D_ == 0) ? 1 : (D_ == 1) ? Nq : Nq * Nq;
+    const int pn = nm + (side ? -(Nq - 1) : (Nq - 1)) * stride_d;
+    const size_t pid = (size_t)nb * Np + pn;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) qp[s] = __ldg(A.q[s] + pid);
+#pragma unroll
+    for (int k = 0; k < NAM; ++k) ap[k] = (k < naux) ? __ldg(A.aux + k * A.stride + pid) : 0.0;
+  } else {
+    boundary_state<LAW, DIM>(L, D_, sgn, -nb, qm, qp);
+#pragma unroll
+    for (int k = 0; k < NAM; ++k) ap[k] = am[k];
+  }
+  double nf[NS];
+  surface_flux<LAW, DIM>(L, A.sflux, D_, sgn, qm, am, qp, ap, nf);
+  const double lift = gid * lift_end;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) ss[(face * Nfp + j) * NS + s] = lift * nf[s];
+}
+
+// NQ_ > 0: the node count per direction is a compile-time constant (index
+// arithmetic folds, line loops unroll); NQ_ = 0 reads it from the arguments.
+template <int LAW, int DIM, int VK, int NQ_>
 __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
   constexpr int NS = NSt<LAW, DIM>::v;
   constexpr int NPRE = NPre<LAW, DIM, VK>::v;
   constexpr int NAM = NAuxMax<LAW, DIM>::v;
   constexpr bool PAIRS = (VK == VK_EC || VK == VK_KG);
   constexpr int NPV = PAIRS ? NPairVals<LAW, DIM, VK>::v : 0;
+  constexpr int NPVS = PAIRS ? NPairVals<LAW, DIM, VK>::stride : 0;
+  constexpr bool CQ = NQ_ > 0;
   extern __shared__ double sm[];
-  const int Nq = A.Nq, Np = A.Np, Nfp = A.Nfp, naux = A.naux;
+  const int Nq = CQ ? NQ_ : A.Nq;
+  const int Np = CQ ? ipow(NQ_, DIM) : A.Np;
+  const int Nfp = CQ ? ipow(NQ_, DIM - 1) : A.Nfp;
+  const int naux = A.naux;
   const int npl = Nq * (Nq - 1) / 2;
   const int slot = threadIdx.x / Np;
   const int node = threadIdx.x - slot * Np;
@@ -97,7 +236,7 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
   const int tabn = 2 * Nq * Nq + 2;
   double* sC = sm;            // Cfd
   double* sW = sm + Nq * Nq;  // Cw
-  const size_t slotsz = (size_t)(NS + naux + NPRE) * Np + (size_t)2 * DIM * Nfp * NS + (size_t)Nfp * npl * NPV;
+  const size_t slotsz = (size_t)(NS + naux + NPRE) * Np + (size_t)2 * DIM * Nfp * NS + (size_t)Nfp * npl * NPVS;
   double* sq = sm + tabn + slot * slotsz;
   double* sa = sq + NS * Np;
   double* sp = sa + naux * Np;
@@ -127,14 +266,26 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
         an[k] = __ldg(A.aux + k * A.stride + gid);
         sa[k * Np + node] = an[k];
       }
-    if constexpr (PAIRS) {
-      if constexpr (LAW == LAW_SW) {
+    if constexpr (VK == VK_EC && LAW == LAW_SW) {
 #pragma unroll
-        for (int c = 0; c < DIM; ++c) Pn[c] = qn[1 + c] / qn[0];
-        Pn[DIM] = qn[DIM + 1] / qn[0];
-      } else {
-        precompute_euler<DIM>(L.gamma, qn, (LAW == LAW_EG) ? an[0] : 0.0, Pn);
-      }
+      for (int c = 0; c < DIM; ++c) Pn[c] = qn[1 + c] / qn[0];
+      Pn[DIM] = qn[DIM + 1] / qn[0];
+    } else if constexpr (VK == VK_EC) {
+      const double rho = qn[0];
+      const double p = pressure_eg<DIM>(L.gamma, qn, (LAW == LAW_EG) ? an[0] : 0.0);
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) Pn[c] = qn[1 + c] / rho;
+      Pn[DIM] = rho / (2.0 * p);
+      Pn[DIM + 1] = dot<DIM>(Pn, Pn);
+      Pn[DIM + 2] = p / rho;
+    } else if constexpr (VK == VK_KG) {
+      const double rho = qn[0];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) Pn[c] = qn[1 + c] / rho;
+      Pn[DIM] = pressure_eg<DIM>(L.gamma, qn, (LAW == LAW_EG) ? an[0] : 0.0);
+      Pn[DIM + 1] = qn[DIM + 1] / rho;
+    }
+    if constexpr (PAIRS) {
 #pragma unroll
       for (int k = 0; k < NPRE; ++k) sp[k * Np + node] = Pn[k];
     } else {
@@ -153,6 +304,7 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
   double T[NS];
 #pragma unroll
   for (int s = 0; s < NS; ++s) T[s] = 0.0;
+  const double igm1 = 1.0 / (L.gamma - 1.0);
   const int ijk[3] = {node % Nq, (node / Nq) % Nq, node / (Nq * Nq)};
   double gi[3] = {0, 0, 0};
   if (act) {
@@ -174,28 +326,22 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
           const int lb = (d == 0) ? line * Nq : (d == 1) ? (line % Nq) + Nq * Nq * (line / Nq) : line;
           const int ab = spair[p];
           const int na = lb + (ab & 0xff) * sd, nb = lb + (ab >> 8) * sd;
-          double f[NPV];
+          double f[NS + 1];
+          double P1[NPRE], P2[NPRE];
+#pragma unroll
+          for (int k = 0; k < NPRE; ++k) { P1[k] = sp[k * Np + na]; P2[k] = sp[k * Np + nb]; }
           if constexpr (LAW == LAW_SW) {
-            double q1[NS], q2[NS], P1[DIM + 1], P2[DIM + 1];
+            double q1[NS], q2[NS];
 #pragma unroll
             for (int s = 0; s < NS; ++s) { q1[s] = sq[s * Np + na]; q2[s] = sq[s * Np + nb]; }
-#pragma unroll
-            for (int k = 0; k < DIM + 1; ++k) { P1[k] = sp[k * Np + na]; P2[k] = sp[k * Np + nb]; }
             sw_ec_dir<DIM>(L.grav, 0, d, q1, P1, 0.0, q2, P2, 0.0, f);
-          } else {
-            double P1[NPRE], P2[NPRE];
-#pragma unroll
-            for (int k = 0; k < NPRE; ++k) { P1[k] = sp[k * Np + na]; P2[k] = sp[k * Np + nb]; }
+          } else if constexpr (VK == VK_EC) {
             const double Phi1 = (LAW == LAW_EG) ? sa[na] : 0.0, Phi2 = (LAW == LAW_EG) ? sa[nb] : 0.0;
-            if constexpr (VK == VK_EC) {
-              double x;
-              ec_sym_dir<LAW, DIM>(L.gamma, d, sq[na], P1, Phi1, sq[nb], P2, Phi2, f, &x);
-              if constexpr (NPV > NS) f[NS] = x;
-            } else {
-              kg_dir<LAW_EULER, DIM>(d, sq[na], P1, 0.0, sq[nb], P2, 0.0, f);
-            }
+            ec_vol<LAW, DIM>(L.gamma, igm1, d, sq[na], P1, Phi1, sq[nb], P2, Phi2, f, f + NS);
+          } else {
+            kg_vol<DIM>(d, sq[na], P1, sq[nb], P2, f);
           }
-          double* dst = spv + (size_t)t * NPV;
+          double* dst = spv + (size_t)t * NPVS;
 #pragma unroll
           for (int s = 0; s < NPV; ++s) dst[s] = f[s];
         }
@@ -204,11 +350,13 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
       // ---- phase B: every node contracts its row, adding its own fluctuation
       if (act) {
         const int line = (d == 0) ? node / Nq : (d == 1) ? ijk[0] + Nq * ijk[2] : node % (Nq * Nq);
-        const double* lp = spv + (size_t)line * npl * NPV;
-        for (int m = 0; m < Nq; ++m) {
+        const double* lp = spv + (size_t)line * npl * NPVS;
+#pragma unroll
+        for (int m = 0; m < (CQ ? NQ_ : 8); ++m) {
+          if (!CQ && m >= Nq) break;
           if (m == id) continue;
           const int p = (m < id) ? pair_index(m, id, Nq) : pair_index(id, m, Nq);
-          const double* fv = lp + p * NPV;
+          const double* fv = lp + p * NPVS;
           double f[NS];
 #pragma unroll
           for (int s = 0; s < NS; ++s) f[s] = fv[s];
@@ -216,7 +364,7 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
           if constexpr (LAW == LAW_EG) {
             const double dPhi = an[0] - sa[nn];
             if constexpr (VK == VK_EC)
-              f[1 + d] = f[1 + d] - fv[NS] * Pn[DIM + 4] * dPhi;  // alpha = b_avg rho_log / (2 b_own)
+              f[1 + d] = f[1 + d] - fv[NS] * Pn[DIM + 2] * dPhi;  // alpha = b_avg rho_log / (2 b_own)
             else
               f[1 + d] = f[1 + d] - ((qn[0] + sq[nn]) / 2.0 / 2.0) * dPhi;
           }
@@ -230,7 +378,9 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
       }
       __syncthreads();  // the pair buffer is reused by the next direction
     } else if (act) {
-      for (int m = 0; m < Nq; ++m) {
+#pragma unroll
+      for (int m = 0; m < (CQ ? NQ_ : 8); ++m) {
+        if (!CQ && m >= Nq) break;
         const int nn = base + m * sd;
         if constexpr (VK == VK_WEAK) {
           const double c = sW[id * Nq + m] * gi[d];
@@ -248,43 +398,17 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
   }
 
   // ------------------------------------------------------------ faces
-  const double lift_end = sm[2 * Nq * Nq];
+  // the face direction is dispatched to a compile-time constant so every
+  // state / normal index in the numerical flux is static (no local memory)
   if (act) {
+    const double lift_end = sm[2 * Nq * Nq];
     for (int t = node; t < 2 * DIM * Nfp; t += Np) {
-      const int face = t / Nfp, j = t - face * Nfp;
-      const int d = face >> 1, side = face & 1;
-      if (!((A.dirs >> d) & 1)) continue;
-      const int t0 = j % Nq, t1 = j / Nq;
-      int fi0, fi1, fi2;
-      if (d == 0) { fi0 = side ? Nq - 1 : 0; fi1 = t0; fi2 = t1; }
-      else if (d == 1) { fi0 = t0; fi1 = side ? Nq - 1 : 0; fi2 = t1; }
-      else { fi0 = t0; fi1 = t1; fi2 = side ? Nq - 1 : 0; }
-      const int nm = fi0 + Nq * (fi1 + Nq * fi2);
-      double qm[NS], qp[NS], am[NAM], ap[NAM];
-#pragma unroll
-      for (int s = 0; s < NS; ++s) qm[s] = sq[s * Np + nm];
-#pragma unroll
-      for (int k = 0; k < NAM; ++k) am[k] = (k < naux) ? sa[k * Np + nm] : 0.0;
-      const int nb = __ldg(A.nbr + 6 * e + face);
-      const double sgn = side ? 1.0 : -1.0;
-      if (nb >= 0) {
-        const int flip = (Nq - 1) * (side ? -1 : 1);
-        const int pn = nm + flip * ((d == 0) ? 1 : (d == 1) ? Nq : Nq * Nq);
-        const size_t pid = (size_t)nb * Np + pn;
-#pragma unroll
-        for (int s = 0; s < NS; ++s) qp[s] = __ldg(A.q[s] + pid);
-#pragma unroll
-        for (int k = 0; k < NAM; ++k) ap[k] = (k < naux) ? __ldg(A.aux + k * A.stride + pid) : 0.0;
-      } else {
-        boundary_state<LAW, DIM>(L, d, sgn, -nb, qm, qp);
-#pragma unroll
-        for (int k = 0; k < NAM; ++k) ap[k] = am[k];
+      const int face = t / Nfp;
+      switch (face >> 1) {
+        case 0: face_task<LAW, DIM, NAM, 0>(A, L, Nq, Np, Nfp, e, t, sq, sa, ss, gi[0], lift_end); break;
+        case 1: if constexpr (DIM > 1) face_task<LAW, DIM, NAM, 1>(A, L, Nq, Np, Nfp, e, t, sq, sa, ss, gi[1], lift_end); break;
+        default: if constexpr (DIM > 2) face_task<LAW, DIM, NAM, 2>(A, L, Nq, Np, Nfp, e, t, sq, sa, ss, gi[2], lift_end); break;
       }
-      double nf[NS];
-      surface_flux<LAW, DIM>(L, A.sflux, d, sgn, qm, am, qp, ap, nf);
-      const double lift = gi[d] * lift_end;
-#pragma unroll
-      for (int s = 0; s < NS; ++s) ss[(face * Nfp + j) * NS + s] = lift * nf[s];
     }
   }
   __syncthreads();
@@ -338,27 +462,31 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
 // launcher signature used by the host dispatch table
 typedef void (*tend_launch_fn)(const TendArgs& A, int grid, int block, size_t smem, cudaStream_t st);
 
-template <int LAW, int DIM, int VK>
+template <int LAW, int DIM, int VK, int NQ_ = 0>
 void tend_launch(const TendArgs& A, int grid, int block, size_t smem, cudaStream_t st) {
   static size_t configured = 0;
   if (smem > 48 * 1024 && smem > configured) {
-    cudaFuncSetAttribute(tendency_kernel<LAW, DIM, VK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(tendency_kernel<LAW, DIM, VK, NQ_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     configured = smem;
   }
-  tendency_kernel<LAW, DIM, VK><<<grid, block, smem, st>>>(A);
+  tendency_kernel<LAW, DIM, VK, NQ_><<<grid, block, smem, st>>>(A);
 }
 
+// generic (runtime Nq) launcher, and the compile-time-Nq specialisations
+// that exist for (law, dim, vk, nq) -- nullptr when there is none
 template <int LAW> tend_launch_fn pick_launcher(int dim, int vk);
+template <int LAW> tend_launch_fn pick_launcher_nq(int dim, int vk, int nq);
 
 // per-node precomputed values and per-pair stored values, for the host
 inline int npre_of(int law, int dim, int vk) {
   int ns = (law == LAW_ADV) ? 1 : dim + 2;
-  if (vk == VK_EC || vk == VK_KG) return (law == LAW_SW) ? dim + 1 : dim + 5;
+  if (vk == VK_EC) return (law == LAW_SW) ? dim + 1 : dim + 3;
+  if (vk == VK_KG) return dim + 2;
   return dim * ns;
 }
-inline int npv_of(int law, int dim, int vk) {
+inline int npv_stride_of(int law, int dim, int vk) {
   int ns = (law == LAW_ADV) ? 1 : dim + 2;
-  if (vk == VK_EC || vk == VK_KG) return ns + ((law == LAW_EG && vk == VK_EC) ? 1 : 0);
+  if (vk == VK_EC || vk == VK_KG) return (ns + ((law == LAW_EG && vk == VK_EC) ? 1 : 0)) | 1;
   return 0;
 }
 
