@@ -278,7 +278,8 @@ extern "C" int atb_op_create(const atb_op_desc* d, const double* aux_host, atb_o
   if (d->dim < 1 || d->dim > 3) return fail(ATB_ERR_INVALID, "dim must be 1..3");
   if (d->N < 1 || d->N > 7) return fail(ATB_ERR_INVALID, "polynomial order N must be 1..7");
   if (d->law < 0 || d->law > 4) return fail(ATB_ERR_INVALID, "unknown law %d", d->law);
-  if (d->precision != ATB_PREC_FP64) return fail(ATB_ERR_INVALID, "precision %d is not built", d->precision);
+  if (d->precision != ATB_PREC_FP64 && d->precision != ATB_PREC_FP32FLUX)
+    return fail(ATB_ERR_INVALID, "unknown precision %d", d->precision);
   if (!d->lgl_weights || !d->lgl_D) return fail(ATB_ERR_INVALID, "LGL tables missing");
   if (d->naux < 0 || d->naux > 8) return fail(ATB_ERR_INVALID, "naux must be 0..8");
   if (d->naux > 0 && !aux_host) return fail(ATB_ERR_INVALID, "aux fields missing");
@@ -288,11 +289,16 @@ extern "C" int atb_op_create(const atb_op_desc* d, const double* aux_host, atb_o
   if (d->volume_form == 1) {
     switch (d->volume_flux) {
       case ATB_FLUX_CENTRAL: vk = VK_CENTRAL; break;
-      case ATB_FLUX_EC: vk = VK_EC; break;
+      case ATB_FLUX_EC: vk = (d->precision == ATB_PREC_FP32FLUX) ? VK_EC32 : VK_EC; break;
       case ATB_FLUX_KG: vk = VK_KG; break;
       default: return fail(ATB_ERR_INVALID, "no two-point volume flux %d", d->volume_flux);
     }
   }
+  if (d->precision == ATB_PREC_FP32FLUX &&
+      !(vk == VK_EC32 && (d->law == LAW_EULER || d->law == LAW_EG || d->law == LAW_SW)))
+    return fail(ATB_ERR_INVALID,
+                "the FP32-flux form exists for the entropy-conservative flux-differencing volume term of "
+                "Euler, Euler-gravity and shallow water");
   tend_launch_fn fn = nullptr;
   red_launch_fn rf = nullptr;
   // a compile-time node-count specialisation when one exists, else the

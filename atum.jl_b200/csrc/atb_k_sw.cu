@@ -13,6 +13,9 @@ template <> tend_launch_fn pick_launcher<LAW_SW>(int dim, int vk) {
   if (dim == 3 && vk == VK_WEAK) return tend_launch<LAW_SW, 3, VK_WEAK, 0>;
   if (dim == 3 && vk == VK_CENTRAL) return tend_launch<LAW_SW, 3, VK_CENTRAL, 0>;
   if (dim == 3 && vk == VK_EC) return tend_launch<LAW_SW, 3, VK_EC, 0>;
+  if (dim == 1 && vk == VK_EC32) return tend_launch<LAW_SW, 1, VK_EC32, 0>;
+  if (dim == 2 && vk == VK_EC32) return tend_launch<LAW_SW, 2, VK_EC32, 0>;
+  if (dim == 3 && vk == VK_EC32) return tend_launch<LAW_SW, 3, VK_EC32, 0>;
   return nullptr;
 }
 template <> red_launch_fn pick_reducer<LAW_SW>(int dim) {

@@ -358,12 +358,66 @@ __device__ __forceinline__ void boundary_state(const LawP& L, int d, T sgn, int 
   }
 }
 
+// Physical flux row d and wave speed of Euler / Euler-gravity / shallow water
+// from one reciprocal 1/rho (the reference recomputes rho u_c / rho in every
+// flux row and in the wave speed; the values agree to an ulp).
+template <int LAW, int DIM, class T>
+__device__ __forceinline__ T flux_ws_recip(const LawP& L, int d, const T* q, const T* aux, T* f) {
+  const T rinv = T(1) / q[0];
+  T u[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) u[c] = q[1 + c] * rinv;
+  if constexpr (LAW == LAW_SW) {
+    const T p = T(L.grav) * (q[0] * q[0]) / T(2);
+    f[0] = q[1 + d];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) f[1 + c] = q[1 + d] * u[c];
+    f[1 + d] = f[1 + d] + p;
+    f[DIM + 1] = u[d] * q[DIM + 1];
+    return fabs(u[d]) + dsqrt(T(L.grav) * q[0]);
+  } else {
+    const T Phi = (LAW == LAW_EG) ? aux[0] : T(0);
+    const T g = T(L.gamma);
+    const T p = (g - T(1)) * (q[DIM + 1] - dot<DIM>(q + 1, u) / T(2) - q[0] * Phi);
+    T dp = p;
+    if (LAW == LAW_EG && L.pde) dp = dp - aux[DIM + 2];
+    f[0] = q[1 + d];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) f[1 + c] = q[1 + d] * u[c];
+    f[1 + d] = f[1 + d] + dp;
+    f[DIM + 1] = u[d] * (q[DIM + 1] + p);
+    return fabs(u[d]) + dsqrt(g * p * rinv);
+  }
+}
+
 // ------------------------------------------------------------ surface flux
 // normal n = sgn * e_d; nf = numerical flux . n (length NS)
 template <int LAW, int DIM, class T>
 __device__ __forceinline__ void surface_flux(const LawP& L, int kind, int d, T sgn, const T* qm, const T* am,
                                              const T* qp, const T* ap, T* nf) {
   constexpr int NS = NSt<LAW, DIM>::v;
+  if constexpr (LAW == LAW_EULER || LAW == LAW_EG || LAW == LAW_SW) {
+    if (kind == F_CENTRAL || kind == F_RUSANOV) {
+      // src/numericalfluxes.jl:31-42 with one reciprocal per side
+      T fm[NS], fp[NS];
+      const T wm = flux_ws_recip<LAW, DIM>(L, d, qm, am, fm);
+      const T wp = flux_ws_recip<LAW, DIM>(L, d, qp, ap, fp);
+#pragma unroll
+      for (int s = 0; s < NS; ++s) nf[s] = ((fm[s] + fp[s]) / T(2)) * sgn;
+      if (kind == F_RUSANOV) {
+        const T ws = dmax(wm, wp);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) nf[s] = nf[s] - ws * (qp[s] - qm[s]) / T(2);
+      }
+      if constexpr (LAW == LAW_SW) {
+        if (L.swtopo) {  // non-conservative surface term g h- (b+ - b-)/2 n
+          const T t = T(L.grav) * qm[0] * (ap[0] - am[0]) / T(2);
+          nf[1 + d] = nf[1 + d] + t * sgn;
+        }
+      }
+      return;
+    }
+  }
   if (kind == F_CENTRAL || kind == F_RUSANOV) {
     T fm[NS], fp[NS];
     flux_dir<LAW, DIM>(L, d, qm, am, fm);

@@ -37,7 +37,9 @@
 
 namespace atb {
 
-enum { VK_WEAK = 0, VK_CENTRAL = 1, VK_EC = 2, VK_KG = 3 };
+// VK_EC32: the entropy-conservative volume flux in the FP32-flux precision
+// form (mixed: balance-critical terms in FP64 adds/multiplies, the rest FP32)
+enum { VK_WEAK = 0, VK_CENTRAL = 1, VK_EC = 2, VK_KG = 3, VK_EC32 = 4 };
 enum { EPI_SET = 0, EPI_ADD = 1, EPI_LSRK = 2, EPI_SUBOUT2 = 3, EPI_RLSRK = 4 };
 
 struct TendArgs {
@@ -60,9 +62,15 @@ struct TendArgs {
 //   KG: u (DIM), p, e = rho e / rho
 //   EC (shallow water): u (DIM), theta
 //   weak / central forms: the DIM physical flux rows (DIM * NS)
+//   EC32 (Euler / Euler-gravity): FP64 p, b, p/rho, then FP32 u (DIM), |u|^2
+//         packed two per double slot
+//   EC32 (shallow water): FP32 u (DIM), theta, packed
 template <int LAW, int DIM, int VK> struct NPre {
   static constexpr int NS = NSt<LAW, DIM>::v;
-  static constexpr int v = (VK == VK_EC) ? ((LAW == LAW_SW) ? DIM + 1 : DIM + 3) : (VK == VK_KG) ? DIM + 2 : DIM * NS;
+  static constexpr int v = (VK == VK_EC)     ? ((LAW == LAW_SW) ? DIM + 1 : DIM + 3)
+                           : (VK == VK_KG)   ? DIM + 2
+                           : (VK == VK_EC32) ? ((LAW == LAW_SW) ? (DIM + 2) / 2 : 3 + (DIM + 2) / 2)
+                                             : DIM * NS;
 };
 // upper bound of the aux components a kernel stages (compile time, so the
 // per-thread aux arrays stay in registers)
@@ -73,7 +81,7 @@ template <int LAW, int DIM> struct NAuxMax {
 // b_avg * rho_log for the Euler-gravity EC fluctuation; the stride is odd so
 // that consecutive pairs fall in different shared-memory banks
 template <int LAW, int DIM, int VK> struct NPairVals {
-  static constexpr int v = NSt<LAW, DIM>::v + ((LAW == LAW_EG && VK == VK_EC) ? 1 : 0);
+  static constexpr int v = NSt<LAW, DIM>::v + ((LAW == LAW_EG && (VK == VK_EC || VK == VK_EC32)) ? 1 : 0);
   static constexpr int stride = v | 1;
 };
 
@@ -150,6 +158,74 @@ __device__ __forceinline__ void ec_vol(T gamma, T igm1, int d, T r1, const T* P1
   *xtra = b_avg * rho_log;
 }
 
+// EC flux, row d, FP32-flux precision form.  Inputs: FP64 rho, p, b and the
+// geopotential; FP32 velocities and |u|^2.  The pressure-like term is the
+// FP64 average of the two pressures plus a second-order FP32 correction,
+//   rho_avg / (2 b_avg) = p_avg - (p1 - p2)(b2 - b1) / (2 (b1 + b2)),
+// and the logarithmic mean of rho is the FP64 average minus a small FP32
+// series correction, so the hydrostatic balance between the pressure and
+// gravity terms is carried in FP64 while every division, logarithm and
+// advective product is FP32.  Returns FP64 row values and b_avg * rho_log.
+template <int LAW, int DIM>
+__device__ __forceinline__ void ec_vol32(float igm1, int d, double r1, double p1, double b1, const float* u1,
+                                         float uu1, double Phi1, double r2, double p2, double b2,
+                                         const float* u2, float uu2, double Phi2, double* f, double* xtra) {
+  const double rho_avg = (r1 + r2) * 0.5, p_avg = (p1 + p2) * 0.5, b_avg = (b1 + b2) * 0.5;
+  const float rs = (float)(r1 + r2), rd = (float)(r1 - r2);
+  const float bs = (float)(b1 + b2), bd = (float)(b1 - b2);
+  const float fr = rd / rs, fb = bd / bs;
+  const float ur = fr * fr, ub = fb * fb;
+  double rho_log;
+  float cterm;
+  if (ur < 1e-4f && ub < 1e-4f) {
+    // 1 - G(u) = u/3 + 4u^2/45 + 44u^3/945 + ...
+    const float cr = ur * (1.f / 3.f + ur * (4.f / 45.f + ur * (44.f / 945.f)));
+    rho_log = rho_avg - rho_avg * (double)cr;
+    cterm = series_F(ub) * igm1 / bs;  // 1 / (2 (gamma-1) b_log)
+  } else {
+    rho_log = logavg_fast(r1, r2);
+    const float b_log = (ub < 1e-4f) ? 0.5f * bs * series_G(ub) : bd / logf((float)b1 / (float)b2);
+    cterm = 0.5f * igm1 / b_log;
+  }
+  const double corr = (double)((float)(p1 - p2) * (float)(b2 - b1) / (2.f * bs));
+  const double pc = p_avg - corr;
+  float ua[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) ua[c] = 0.5f * (u1[c] + u2[c]);
+  const float rl = (float)rho_log;
+  const float ud = ua[d];
+  const float frd = ud * rl;
+  f[0] = (double)frd;
+  float mu = 0.f;
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    const float m = ud * (ua[c] * rl);
+    f[1 + c] = (double)m;
+    mu += m * ua[c];
+  }
+  f[1 + d] += pc;
+  mu += (float)pc * ud;
+  float c1 = cterm - 0.25f * (uu1 + uu2);
+  if (LAW == LAW_EG) c1 += (float)((Phi1 + Phi2) * 0.5);
+  f[DIM + 1] = (double)(c1 * frd + mu);
+  *xtra = b_avg * rho_log;
+}
+
+// shallow-water EC flux, row d, FP32-flux form: the pressure term
+// g (rho_avg^2 - rho2_avg/2) = g rho1 rho2 / 2 stays FP64, advective products
+// are FP32
+template <int DIM>
+__device__ __forceinline__ void sw_vol32(double grav, int d, const double* q1, const float* P1, const double* q2,
+                                         const float* P2, double* f) {
+  const double md = 0.5 * (q1[1 + d] + q2[1 + d]);
+  const float mdf = (float)md;
+  f[0] = md;
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) f[1 + c] = (double)(mdf * (0.5f * (P1[c] + P2[c])));
+  f[1 + d] += grav * q1[0] * q2[0] * 0.5;
+  f[DIM + 1] = (double)(mdf * (0.5f * (P1[DIM] + P2[DIM])));
+}
+
 template <int DIM, class T>
 __device__ __forceinline__ void kg_vol(int d, T r1, const T* P1, T r2, const T* P2, T* f) {
   const T rho_avg = (r1 + r2) / T(2);
@@ -219,7 +295,8 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
   constexpr int NS = NSt<LAW, DIM>::v;
   constexpr int NPRE = NPre<LAW, DIM, VK>::v;
   constexpr int NAM = NAuxMax<LAW, DIM>::v;
-  constexpr bool PAIRS = (VK == VK_EC || VK == VK_KG);
+  constexpr bool PAIRS = (VK == VK_EC || VK == VK_KG || VK == VK_EC32);
+  constexpr int PR_IDX = (VK == VK_EC32) ? 2 : DIM + 2;  // p/rho in the own-node values
   constexpr int NPV = PAIRS ? NPairVals<LAW, DIM, VK>::v : 0;
   constexpr int NPVS = PAIRS ? NPairVals<LAW, DIM, VK>::stride : 0;
   constexpr bool CQ = NQ_ > 0;
@@ -271,21 +348,53 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
       for (int c = 0; c < DIM; ++c) Pn[c] = qn[1 + c] / qn[0];
       Pn[DIM] = qn[DIM + 1] / qn[0];
     } else if constexpr (VK == VK_EC) {
-      const double rho = qn[0];
-      const double p = pressure_eg<DIM>(L.gamma, qn, (LAW == LAW_EG) ? an[0] : 0.0);
+      // one reciprocal of rho and one of p/rho per node
+      const double rho = qn[0], rinv = 1.0 / rho;
 #pragma unroll
-      for (int c = 0; c < DIM; ++c) Pn[c] = qn[1 + c] / rho;
-      Pn[DIM] = rho / (2.0 * p);
+      for (int c = 0; c < DIM; ++c) Pn[c] = qn[1 + c] * rinv;
+      const double Phi = (LAW == LAW_EG) ? an[0] : 0.0;
+      const double p = (L.gamma - 1.0) * (qn[DIM + 1] - dot<DIM>(qn + 1, Pn) / 2.0 - rho * Phi);
+      const double pr = p * rinv;
+      Pn[DIM] = 0.5 / pr;  // b = rho / (2 p)
       Pn[DIM + 1] = dot<DIM>(Pn, Pn);
-      Pn[DIM + 2] = p / rho;
+      Pn[DIM + 2] = pr;
     } else if constexpr (VK == VK_KG) {
       const double rho = qn[0];
 #pragma unroll
       for (int c = 0; c < DIM; ++c) Pn[c] = qn[1 + c] / rho;
       Pn[DIM] = pressure_eg<DIM>(L.gamma, qn, (LAW == LAW_EG) ? an[0] : 0.0);
       Pn[DIM + 1] = qn[DIM + 1] / rho;
+    } else if constexpr (VK == VK_EC32 && LAW == LAW_SW) {
+      float* spf = (float*)sp;
+      const float hinv = 1.f / (float)qn[0];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) spf[c * Np + node] = (float)qn[1 + c] * hinv;
+      spf[DIM * Np + node] = (float)qn[DIM + 1] * hinv;
+    } else if constexpr (VK == VK_EC32) {
+      const double rho = qn[0], rinv = 1.0 / rho;
+      const double Phi = (LAW == LAW_EG) ? an[0] : 0.0;
+      const double ke = 0.5 * dot<DIM>(qn + 1, qn + 1) * rinv;
+      const double p = (L.gamma - 1.0) * (qn[DIM + 1] - ke - rho * Phi);
+      const double pr = p * rinv;
+      Pn[0] = p;
+      Pn[1] = 0.5 / pr;
+      Pn[2] = pr;
+      float* spf = (float*)(sp + 3 * Np);
+      const float rinvf = (float)rinv;
+      float uu = 0.f;
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        const float u = (float)qn[1 + c] * rinvf;
+        spf[c * Np + node] = u;
+        uu += u * u;
+      }
+      spf[DIM * Np + node] = uu;
     }
-    if constexpr (PAIRS) {
+    if constexpr (VK == VK_EC32 && LAW != LAW_SW) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) sp[k * Np + node] = Pn[k];
+    } else if constexpr (VK == VK_EC32) {
+    } else if constexpr (PAIRS) {
 #pragma unroll
       for (int k = 0; k < NPRE; ++k) sp[k * Np + node] = Pn[k];
     } else {
@@ -327,6 +436,30 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
           const int ab = spair[p];
           const int na = lb + (ab & 0xff) * sd, nb = lb + (ab >> 8) * sd;
           double f[NS + 1];
+          if constexpr (VK == VK_EC32) {
+            if constexpr (LAW == LAW_SW) {
+              const float* spf = (const float*)sp;
+              float P1[DIM + 1], P2[DIM + 1];
+              double q1[NS], q2[NS];
+#pragma unroll
+              for (int k = 0; k < DIM + 1; ++k) { P1[k] = spf[k * Np + na]; P2[k] = spf[k * Np + nb]; }
+#pragma unroll
+              for (int s = 0; s < NS; ++s) { q1[s] = sq[s * Np + na]; q2[s] = sq[s * Np + nb]; }
+              sw_vol32<DIM>(L.grav, d, q1, P1, q2, P2, f);
+            } else {
+              const float* spf = (const float*)(sp + 3 * Np);
+              float u1[DIM], u2[DIM];
+#pragma unroll
+              for (int c = 0; c < DIM; ++c) { u1[c] = spf[c * Np + na]; u2[c] = spf[c * Np + nb]; }
+              const double Phi1 = (LAW == LAW_EG) ? sa[na] : 0.0, Phi2 = (LAW == LAW_EG) ? sa[nb] : 0.0;
+              ec_vol32<LAW, DIM>((float)igm1, d, sq[na], sp[na], sp[Np + na], u1, spf[DIM * Np + na], Phi1, sq[nb],
+                                 sp[nb], sp[Np + nb], u2, spf[DIM * Np + nb], Phi2, f, f + NS);
+            }
+            double* dst = spv + (size_t)t * NPVS;
+#pragma unroll
+            for (int s = 0; s < NPV; ++s) dst[s] = f[s];
+            continue;
+          }
           double P1[NPRE], P2[NPRE];
 #pragma unroll
           for (int k = 0; k < NPRE; ++k) { P1[k] = sp[k * Np + na]; P2[k] = sp[k * Np + nb]; }
@@ -363,8 +496,8 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
           const int nn = base + m * sd;
           if constexpr (LAW == LAW_EG) {
             const double dPhi = an[0] - sa[nn];
-            if constexpr (VK == VK_EC)
-              f[1 + d] = f[1 + d] - fv[NS] * Pn[DIM + 2] * dPhi;  // alpha = b_avg rho_log / (2 b_own)
+            if constexpr (VK == VK_EC || VK == VK_EC32)
+              f[1 + d] = f[1 + d] - fv[NS] * Pn[PR_IDX] * dPhi;  // alpha = b_avg rho_log / (2 b_own)
             else
               f[1 + d] = f[1 + d] - ((qn[0] + sq[nn]) / 2.0 / 2.0) * dPhi;
           }
@@ -480,13 +613,15 @@ template <int LAW> tend_launch_fn pick_launcher_nq(int dim, int vk, int nq);
 // per-node precomputed values and per-pair stored values, for the host
 inline int npre_of(int law, int dim, int vk) {
   int ns = (law == LAW_ADV) ? 1 : dim + 2;
+  if (vk == VK_EC32) return (law == LAW_SW) ? (dim + 2) / 2 : 3 + (dim + 2) / 2;
   if (vk == VK_EC) return (law == LAW_SW) ? dim + 1 : dim + 3;
   if (vk == VK_KG) return dim + 2;
   return dim * ns;
 }
 inline int npv_stride_of(int law, int dim, int vk) {
   int ns = (law == LAW_ADV) ? 1 : dim + 2;
-  if (vk == VK_EC || vk == VK_KG) return (ns + ((law == LAW_EG && vk == VK_EC) ? 1 : 0)) | 1;
+  if (vk == VK_EC || vk == VK_KG || vk == VK_EC32)
+    return (ns + ((law == LAW_EG && (vk == VK_EC || vk == VK_EC32)) ? 1 : 0)) | 1;
   return 0;
 }
 

@@ -111,7 +111,7 @@ def isentropic_vortex(N=4, K=5, form="weak"):
     return Case(f"isentropic_vortex_{form}_K{K}", dg, vortex(x, 0.0), dt, 5.0, exact=lambda t: vortex(x, t))
 
 
-def vortex_c1(N=3, K=8, steps=100, vflux="ec"):
+def vortex_c1(N=3, K=8, steps=100, vflux="ec", precision="fp64"):
     """Plain-method config: 2-D Euler isentropic vortex on periodic [-5,5]^2,
     8x8 elements, N=3, rho=1, u=v=1, p=1, gamma=1.4, strength 5 at the origin,
     EC volume flux, Rusanov surface flux, LSRK54, dt = 0.3 dx / N, 100 fixed
@@ -121,7 +121,7 @@ def vortex_c1(N=3, K=8, steps=100, vflux="ec"):
     v = _vec(-5.0, 5.0, K)
     grid = A.brickgrid(cell, (v, v), periodic=(True, True))
     vf = A.FluxDifferencingForm(A.EntropyConservativeFlux() if vflux == "ec" else A.KennedyGruberFlux())
-    dg = A.DGSEM(law=law, grid=grid, volume_form=vf, surface_numericalflux=A.RusanovFlux())
+    dg = A.DGSEM(law=law, grid=grid, volume_form=vf, surface_numericalflux=A.RusanovFlux(), precision=precision)
     dx = v[1] - v[0]
     g = law.gamma
 
@@ -285,8 +285,9 @@ def bubble_3d(N=4, K=16, L=10e3, imex=True, steps=200, dt=None, precision="fp64"
     dz = A.min_node_distance(grid, dims=(3,))
     if imex:
         lin = A.LinearEulerGravityLaw(law)
-        lindg = A.DGSEM(law=lin, grid=grid, surface_numericalflux=A.RusanovFlux(), auxstate=aux, directions=(3,),
-                        precision=precision)
+        # the implicit vertical operator and its banded solve stay FP64 in
+        # every precision form
+        lindg = A.DGSEM(law=lin, grid=grid, surface_numericalflux=A.RusanovFlux(), auxstate=aux, directions=(3,))
         # the box is isotropic: the explicit part's horizontal acoustic CFL sets dt
         dt = dt if dt is not None else 0.25 * dz / 340.0
         return Case("bubble_3d_imex", dg, q0, dt, steps * dt, solver="ARK23", lindg=lindg, split_rhs=False,
@@ -307,3 +308,57 @@ def golden(key, form, level=1):
         if v["form"] == form and v["level"] == level:
             return v["value"]
     raise KeyError((key, form, level))
+
+
+# ------------------------------------------------------ shallow water, C3
+def sw_fplane(N=4, K=32, L=1.0e6, H=100.0, seed=20261203, lake_at_rest=False, precision="fp64", f=1e-4,
+              steps=500):
+    """Rotating shallow water (f-plane, g = 9.81) on a periodic square of K x K
+    elements, order N; smooth random bottom topography (sum of 8 Gaussians,
+    amplitude <= 10% of the mean depth H) and seeded random height
+    perturbations (amplitude 1 m, wavelengths 4-16 elements).  EC volume flux
+    with the well-balanced bathymetry terms, Rusanov surface flux, LSRK54."""
+    rng = np.random.default_rng(seed)
+    cell = A.LobattoCell(N + 1, N + 1)
+    v = _vec(0.0, L, K)
+    grid = A.brickgrid(cell, (v, v), periodic=(True, True))
+    g = 9.81
+    cx, cy = rng.uniform(0, L, 8), rng.uniform(0, L, 8)
+    amp = rng.uniform(-0.1 * H, 0.1 * H, 8) / 2
+    wid = rng.uniform(0.05 * L, 0.15 * L, 8)
+
+    def bath(x):
+        b = np.zeros(x.shape[1:])
+        gx, gy = np.zeros_like(b), np.zeros_like(b)
+        for i in range(8):
+            dx = (x[0] - cx[i] + L / 2) % L - L / 2
+            dy = (x[1] - cy[i] + L / 2) % L - L / 2
+            e = amp[i] * np.exp(-(dx * dx + dy * dy) / wid[i] ** 2)
+            b += e
+            gx += -2 * dx / wid[i] ** 2 * e
+            gy += -2 * dy / wid[i] ** 2 * e
+        return b, [gx, gy]
+
+    law = A.ShallowWaterLaw(2, grav=g, topography=True, problem=A.Coriolis((0.0, 0.0, f)))
+    law.bathymetry = bath
+    dg = A.DGSEM(law=law, grid=grid, volume_form=A.FluxDifferencingForm(A.EntropyConservativeFlux()),
+                 surface_numericalflux=A.RusanovFlux(), precision=precision)
+    x = grid.points()
+    b = dg.auxstate_host()[0]
+    eta = np.zeros_like(b)
+    if not lake_at_rest:
+        for _ in range(6):
+            wl = rng.uniform(4, 16) * (L / K)
+            th = rng.uniform(0, 2 * np.pi)
+            kx, ky = 2 * np.pi / wl * np.cos(th), 2 * np.pi / wl * np.sin(th)
+            # periodic: round the wavenumber to the box
+            kx = 2 * np.pi * np.round(kx * L / (2 * np.pi)) / L
+            ky = 2 * np.pi * np.round(ky * L / (2 * np.pi)) / L
+            eta += np.sin(kx * x[0] + ky * x[1] + rng.uniform(0, 2 * np.pi))
+        eta *= 1.0 / np.max(np.abs(eta))
+    h = H - b + eta
+    z = np.zeros_like(h)
+    q0 = _pack(h, z, z, h * 0.0)
+    dx = L / K
+    dt = 0.3 * dx / N / (np.sqrt(g * np.max(h)))
+    return Case("sw_fplane", dg, q0, dt, steps * dt, extra={"steps": steps})

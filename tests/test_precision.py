@@ -1,0 +1,84 @@
+"""FP32-flux precision form against the FP64 path (both on the GPU; the FP64
+path matches the CPU oracle to 1e-12, see test_gpu_parity.py).
+
+The error measure is the reference's own weighted L2 norm (src/measures.jl),
+relative: ||q_fp32flux - q_fp64|| / ||q_fp64||, bound 1e-6.  For the rising
+bubble the error relative to the bubble's perturbation (q - q_background) is
+reported too.
+"""
+import numpy as np
+import pytest
+
+import atum_b200 as A
+import parity as PT
+import problems as P
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(dg, a, b):
+    import torch
+    return A.weightednorm(dg, (a - b).contiguous()) / A.weightednorm(dg, b)
+
+
+def test_bubble_imex_fp32flux(capsys):
+    import torch
+    c64 = P.bubble_3d(N=4, K=6, imex=True, steps=40)
+    c32 = P.bubble_3d(N=4, K=6, imex=True, steps=40, precision="fp32flux")
+    q64, q32 = PT.to_dev(c64.q0), PT.to_dev(c32.q0)
+    s64 = A.ARK23(c64.dg, c64.lindg, q64, c64.dt, split_rhs=False)
+    s32 = A.ARK23(c32.dg, c32.lindg, q32, c32.dt, split_rhs=False)
+    s64.step(q64, 40)
+    s32.step(q32, 40)
+    rel = _rel(c64.dg, q32, q64)
+    # error relative to the perturbation the bubble made
+    qb = PT.to_dev(P.bubble_3d(N=4, K=6, imex=True, steps=1).q0)
+    pert = A.weightednorm(c64.dg, (q64 - qb).contiguous())
+    rel_pert = A.weightednorm(c64.dg, (q32 - q64).contiguous()) / pert
+    with capsys.disabled():
+        print(f"\n  bubble 3-D IMEX, 40 steps: rel L2 {rel:.2e}, rel to perturbation {rel_pert:.2e}")
+    assert rel <= 1e-6
+    assert rel_pert <= 1e-3
+
+
+def test_vortex_fp32flux():
+    c64 = P.vortex_c1()
+    c32 = P.vortex_c1(precision="fp32flux")
+    q64, q32 = PT.to_dev(c64.q0), PT.to_dev(c32.q0)
+    A.LSRK54(c64.dg, q64, c64.dt).step(q64, 100)
+    A.LSRK54(c32.dg, q32, c32.dt).step(q32, 100)
+    assert _rel(c64.dg, q32, q64) <= 1e-6
+
+
+def test_shallow_water_fp32flux_and_mass():
+    import torch
+    c64 = P.sw_fplane(K=8, steps=50)
+    c32 = P.sw_fplane(K=8, steps=50, precision="fp32flux")
+    q64, q32 = PT.to_dev(c64.q0), PT.to_dev(c32.q0)
+    A.LSRK54(c64.dg, q64, c64.dt).step(q64, 50)
+    A.LSRK54(c32.dg, q32, c32.dt).step(q32, 50)
+    assert _rel(c64.dg, q32, q64) <= 1e-6
+    mj = PT.to_dev(c32.dg.MJ)
+    m0 = float((mj * PT.to_dev(c32.q0)[0]).sum())
+    m1 = float((mj * q32[0]).sum())
+    assert abs(m1 - m0) <= 1e-13 * abs(m0)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32flux"])
+def test_lake_at_rest(precision):
+    """Well-balancedness with bathymetry and Coriolis: h + b = const, u = 0
+    stays at rest to round-off."""
+    c = P.sw_fplane(K=8, lake_at_rest=True, precision=precision, steps=20)
+    q = PT.to_dev(c.q0)
+    A.LSRK54(c.dg, q, c.dt).step(q, 20)
+    umax = float(q[1:3].abs().max() / q[0].abs().max())
+    assert umax <= 1e-12, umax
+    assert float((q[0] - PT.to_dev(c.q0)[0]).abs().max()) <= 1e-10
+
+
+def test_fp32flux_rejected_where_not_built():
+    cell = A.LobattoCell(3, 3)
+    grid = A.brickgrid(cell, ([0, 1, 2], [0, 1, 2]), periodic=(True, True))
+    dg = A.DGSEM(law=A.EulerLaw(2), grid=grid, surface_numericalflux=A.RusanovFlux(), precision="fp32flux")
+    with pytest.raises(A._lib.AtbError):
+        dg.device
