@@ -50,6 +50,13 @@ SIGNATURES = {
     "atb_op_create": [C.POINTER(OpDesc), _DP, C.POINTER(C.c_void_p)],
     "atb_op_destroy": [_VP],
     "atb_op_dims": [_VP, _IP, _IP, _IP],
+    "atb_op_create_batch": [C.POINTER(OpDesc), C.c_int, C.POINTER(_DP), C.POINTER(C.c_void_p)],
+    "atb_op_instances": [_VP, _IP, _IP],
+    "atb_op_autotune": [_VP, PtrArr, _DP, _VP, _IP],
+    "atb_op_set_launch": [_VP, C.c_int],
+    "atb_op_set_active": [_VP, C.c_int],
+    "atb_op_set_instance_aux": [_VP, C.c_int, _DP, _VP],
+    "atb_op_copy_instance_aux": [_VP, C.c_int, C.c_int, _VP],
     "atb_op_apply": [_VP, PtrArr, PtrArr, C.c_double, C.c_int, _VP],
     "atb_solver_create": [C.c_int, _VP, _VP, C.c_double, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_void_p)],
     "atb_solver_destroy": [_VP],
@@ -57,6 +64,8 @@ SIGNATURES = {
     "atb_solve": [_VP, PtrArr, C.c_double, C.c_int, _IP, _VP],
     "atb_solver_get": [_VP, _DP, _DP, _DP],
     "atb_solver_set_dt": [_VP, C.c_double],
+    "atb_solver_set_instance_dt": [_VP, _DP],
+    "atb_solver_set_element_dt": [_VP, _DP],
     "atb_weightednorm": [_VP, PtrArr, C.c_double, _DP, _DP, _VP],
     "atb_entropyintegral": [_VP, PtrArr, _DP, _VP],
     "atb_entropyproduct": [_VP, PtrArr, PtrArr, _DP, _VP],

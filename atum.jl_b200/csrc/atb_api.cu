@@ -137,6 +137,12 @@ struct atb_op {
   int dim = 0, N = 0, Nq = 0, Np = 0, Nfp = 0, K = 0, Kd[3] = {1, 1, 1}, ns = 0, naux = 0;
   int vk = 0, dirs = 0, sflux = 0, precision = 0, stacked = 0;
   int naux_used = 0;  // leading aux components the tendency kernel stages
+  int ninst = 1;      // instances packed into this operator
+  int K_active = 0;   // elements the tendency launches cover (a prefix of K)
+  std::vector<int> inst_off;  // first element of each instance, then K
+  std::vector<int> col_e0;    // bottom element of every vertical column
+  bool cols_uniform = true;   // every instance has the same element counts
+  int npre = 0, npv = 0;
   std::vector<double> w, D;
   double* d_ginv = nullptr;
   int* d_nbr = nullptr;
@@ -154,22 +160,16 @@ struct atb_op {
   int E = 1;
   size_t smem = 0;
   size_t stride() const { return (size_t)K * Np; }
-  int elem_of(const int* idx) const {
-    if (stacked) {
-      int ev = idx[dim - 1], eh = 0, m = 1;
-      for (int d = 0; d < dim - 1; ++d) { eh += idx[d] * m; m *= Kd[d]; }
-      return eh * Kd[dim - 1] + ev;
-    }
-    int e = 0, m = 1;
-    for (int d = 0; d < dim; ++d) { e += idx[d] * m; m *= Kd[d]; }
-    return e;
-  }
 };
 
 namespace {
 
+size_t op_smem(const atb_op* op, int E) {
+  return tend_smem_bytes(op->ns, op->npre, op->naux_used, op->dim, op->Nq, op->Np, op->Nfp, E, op->npv);
+}
+
 void fill_args(const atb_op* op, TendArgs& A) {
-  A.K = op->K;
+  A.K = op->K_active;
   A.Nq = op->Nq;
   A.Np = op->Np;
   A.Nfp = op->Nfp;
@@ -185,22 +185,25 @@ void fill_args(const atb_op* op, TendArgs& A) {
   A.stride = op->stride();
   A.a = 0;
   A.bdt = 0;
+  A.dte = nullptr;
 }
 
 // one tendency launch: epi with input q, outputs out/out2
 int run_tendency(atb_op* op, int epi, const double* const* q, double* const* out, double* const* out2, double a,
-                 double bdt, cudaStream_t st) {
+                 double bdt, cudaStream_t st, const double* dte = nullptr) {
   TendArgs A;
   fill_args(op, A);
   A.epi = epi;
   A.a = a;
   A.bdt = bdt;
+  A.dte = dte;
   for (int s = 0; s < 5; ++s) {
     A.q[s] = q[s < op->ns ? s : 0];
     A.out[s] = out ? out[s < op->ns ? s : 0] : nullptr;
     A.out2[s] = out2 ? out2[s < op->ns ? s : 0] : nullptr;
   }
-  int grid = (op->K + op->E - 1) / op->E;
+  int grid = (op->K_active + op->E - 1) / op->E;
+  if (grid == 0) return ATB_OK;
   {
     ProfScope ps(op->prof_class, st);
     op->launch(A, grid, op->E * op->Np, op->smem, st);
@@ -272,9 +275,42 @@ extern "C" int atb_op_destroy(atb_op* op) {
   return ATB_OK;
 }
 
-extern "C" int atb_op_create(const atb_op_desc* d, const double* aux_host, atb_op** out) {
-  if (!d || !out) return fail(ATB_ERR_INVALID, "null argument");
+namespace {
+
+// element number of per-dimension indices idx in one instance's ordering
+int elem_index(const atb_op_desc* d, const int* idx) {
+  if (d->stacked) {
+    int ev = idx[d->dim - 1], eh = 0, m = 1;
+    for (int k = 0; k < d->dim - 1; ++k) { eh += idx[k] * m; m *= d->K[k]; }
+    return eh * d->K[d->dim - 1] + ev;
+  }
+  int e = 0, m = 1;
+  for (int k = 0; k < d->dim; ++k) { e += idx[k] * m; m *= d->K[k]; }
+  return e;
+}
+
+bool same_kind(const atb_op_desc* a, const atb_op_desc* b) {
+  bool ok = a->law == b->law && a->dim == b->dim && a->N == b->N && a->volume_form == b->volume_form &&
+            a->volume_flux == b->volume_flux && a->surface_flux == b->surface_flux && a->directions == b->directions &&
+            a->gamma == b->gamma && a->grav == b->grav && a->sphere == b->sphere &&
+            a->pde_level_balance == b->pde_level_balance && a->bc_kind == b->bc_kind &&
+            a->source_kind == b->source_kind && a->sw_topography == b->sw_topography && a->naux == b->naux &&
+            a->precision == b->precision;
+  for (int k = 0; k < 3; ++k) ok = ok && a->adv_u[k] == b->adv_u[k] && a->omega[k] == b->omega[k];
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 5; ++j) ok = ok && a->bc_state[i][j] == b->bc_state[i][j];
+  return ok;
+}
+
+// One operator over n instances that share their law, order, fluxes,
+// precision and problem kinds: their elements are concatenated (instance i
+// owns elements [off_i, off_i + K_i)) and every neighbour index is offset, so
+// the tendency kernel -- which only sees an element list -- advances all of
+// them in one launch (the instances never couple).
+int op_create_impl(const atb_op_desc* descs, int n, const double* const* aux_hosts, atb_op** out) {
+  if (!descs || !out || n < 1) return fail(ATB_ERR_INVALID, "null argument");
   *out = nullptr;
+  const atb_op_desc* d = &descs[0];
   if (d->dim < 1 || d->dim > 3) return fail(ATB_ERR_INVALID, "dim must be 1..3");
   if (d->N < 1 || d->N > 7) return fail(ATB_ERR_INVALID, "polynomial order N must be 1..7");
   if (d->law < 0 || d->law > 4) return fail(ATB_ERR_INVALID, "unknown law %d", d->law);
@@ -282,9 +318,18 @@ extern "C" int atb_op_create(const atb_op_desc* d, const double* aux_host, atb_o
     return fail(ATB_ERR_INVALID, "unknown precision %d", d->precision);
   if (!d->lgl_weights || !d->lgl_D) return fail(ATB_ERR_INVALID, "LGL tables missing");
   if (d->naux < 0 || d->naux > 8) return fail(ATB_ERR_INVALID, "naux must be 0..8");
-  if (d->naux > 0 && !aux_host) return fail(ATB_ERR_INVALID, "aux fields missing");
   if ((d->directions & ((1 << d->dim) - 1)) == 0 || (d->directions >> d->dim))
     return fail(ATB_ERR_INVALID, "directions must be a non-empty subset of 1:dim");
+  for (int i = 0; i < n; ++i) {
+    if (i > 0 && !same_kind(d, &descs[i]))
+      return fail(ATB_ERR_INVALID, "batched instance %d differs from instance 0 in law, order, fluxes, "
+                                   "precision or problem kinds", i);
+    if (descs[i].naux > 0 && (!aux_hosts || !aux_hosts[i])) return fail(ATB_ERR_INVALID, "aux fields missing");
+    for (int k = 0; k < d->dim; ++k) {
+      if (descs[i].K[k] < 1) return fail(ATB_ERR_INVALID, "K[%d] must be >= 1", k);
+      if (!descs[i].vertices[k]) return fail(ATB_ERR_INVALID, "vertex vector %d missing", k);
+    }
+  }
   int vk = VK_WEAK;
   if (d->volume_form == 1) {
     switch (d->volume_flux) {
@@ -333,15 +378,20 @@ extern "C" int atb_op_create(const atb_op_desc* d, const double* aux_host, atb_o
   op->Np = 1;
   for (int k = 0; k < d->dim; ++k) op->Np *= op->Nq;
   op->Nfp = op->Np / op->Nq;
-  op->K = 1;
-  for (int k = 0; k < 3; ++k) {
-    op->Kd[k] = k < d->dim ? d->K[k] : 1;
-    if (op->Kd[k] < 1) {
-      delete op;
-      return fail(ATB_ERR_INVALID, "K[%d] must be >= 1", k);
-    }
-    op->K *= op->Kd[k];
+  op->ninst = n;
+  op->K = 0;
+  std::vector<int> offs(n + 1, 0);
+  for (int i = 0; i < n; ++i) {
+    int Ki = 1;
+    for (int k = 0; k < d->dim; ++k) Ki *= descs[i].K[k];
+    offs[i + 1] = offs[i] + Ki;
   }
+  op->K = offs[n];
+  op->K_active = op->K;
+  op->inst_off = offs;
+  for (int k = 0; k < 3; ++k) op->Kd[k] = k < d->dim ? d->K[k] : 1;  // instance 0
+  for (int i = 1; i < n; ++i)
+    for (int k = 0; k < d->dim; ++k) op->cols_uniform = op->cols_uniform && descs[i].K[k] == d->K[k];
   op->ns = (d->law == LAW_ADV) ? 1 : d->dim + 2;
   op->naux = d->naux;
   op->vk = vk;
@@ -376,43 +426,58 @@ extern "C" int atb_op_create(const atb_op_desc* d, const double* aux_host, atb_o
       tab[Nq * Nq + i * Nq + m] = cw;
     }
   tab[2 * Nq * Nq] = 1.0 / op->w[0];
-  // geometry
+  // geometry, instance by instance
   std::vector<double> ginv((size_t)K * 3, 0.0), J(K, 1.0);
   std::vector<int> nbr((size_t)K * 6, 0);
-  int idx[3];
-  for (idx[2] = 0; idx[2] < op->Kd[2]; ++idx[2])
-    for (idx[1] = 0; idx[1] < op->Kd[1]; ++idx[1])
-      for (idx[0] = 0; idx[0] < op->Kd[0]; ++idx[0]) {
-        const int e = op->elem_of(idx);
-        double Je = 1.0;
-        for (int k = 0; k < dim; ++k) {
-          const double h = d->vertices[k][idx[k] + 1] - d->vertices[k][idx[k]];
-          if (!(h > 0)) {
-            delete op;
-            return fail(ATB_ERR_INVALID, "vertex vector %d is not increasing", k);
-          }
-          ginv[e * 3 + k] = 2.0 / h;
-          Je *= h / 2;
-        }
-        J[e] = Je;
-        for (int k = 0; k < 3; ++k)
-          for (int f = 0; f < 2; ++f) {
-            int face = 2 * k + f;
-            if (k >= dim) { nbr[e * 6 + face] = -(face + 1); continue; }
-            int nb[3] = {idx[0], idx[1], idx[2]};
-            nb[k] += f ? 1 : -1;
-            if (nb[k] < 0 || nb[k] >= op->Kd[k]) {
-              if (d->periodic[k]) {
-                nb[k] = (nb[k] + op->Kd[k]) % op->Kd[k];
-              } else {
-                nbr[e * 6 + face] = -(face + 1);  // boundary tag = face number
-                continue;
-              }
-            }
-            nbr[e * 6 + face] = op->elem_of(nb);
-          }
+  for (int inst = 0; inst < n; ++inst) {
+    const atb_op_desc* di = &descs[inst];
+    const int off = offs[inst];
+    int Kd[3] = {1, 1, 1};
+    for (int k = 0; k < dim; ++k) Kd[k] = di->K[k];
+    int idx[3];
+    {
+      // vertical columns (last dimension), horizontal element index fastest
+      int KH = 1;
+      for (int k = 0; k < dim - 1; ++k) KH *= Kd[k];
+      for (int eh = 0; eh < KH; ++eh) {
+        int ci[3] = {0, 0, 0}, r = eh;
+        for (int k = 0; k < dim - 1; ++k) { ci[k] = r % Kd[k]; r /= Kd[k]; }
+        op->col_e0.push_back(off + elem_index(di, ci));
       }
-  // launch shape: E elements per CTA, ~256 threads (>= 1 element)
+    }
+    for (idx[2] = 0; idx[2] < Kd[2]; ++idx[2])
+      for (idx[1] = 0; idx[1] < Kd[1]; ++idx[1])
+        for (idx[0] = 0; idx[0] < Kd[0]; ++idx[0]) {
+          const int e = off + elem_index(di, idx);
+          double Je = 1.0;
+          for (int k = 0; k < dim; ++k) {
+            const double h = di->vertices[k][idx[k] + 1] - di->vertices[k][idx[k]];
+            if (!(h > 0)) {
+              delete op;
+              return fail(ATB_ERR_INVALID, "vertex vector %d of instance %d is not increasing", k, inst);
+            }
+            ginv[e * 3 + k] = 2.0 / h;
+            Je *= h / 2;
+          }
+          J[e] = Je;
+          for (int k = 0; k < 3; ++k)
+            for (int f = 0; f < 2; ++f) {
+              int face = 2 * k + f;
+              if (k >= dim) { nbr[e * 6 + face] = -(face + 1); continue; }
+              int nb[3] = {idx[0], idx[1], idx[2]};
+              nb[k] += f ? 1 : -1;
+              if (nb[k] < 0 || nb[k] >= Kd[k]) {
+                if (di->periodic[k]) {
+                  nb[k] = (nb[k] + Kd[k]) % Kd[k];
+                } else {
+                  nbr[e * 6 + face] = -(face + 1);  // boundary tag = face number
+                  continue;
+                }
+              }
+              nbr[e * 6 + face] = off + elem_index(di, nb);
+            }
+        }
+  }
   // aux components the kernels read: Euler-gravity needs Phi (fluxes, wave
   // speeds), grad Phi for the weak form's non-conservative term, and the
   // reference state under pde_level_balance; the linear law needs all of
@@ -422,12 +487,13 @@ extern "C" int atb_op_create(const atb_op_desc* d, const double* aux_host, atb_o
   if (d->law == LAW_LEG) nu = dim + 3;
   if (d->law == LAW_SW && d->sw_topography) nu = (vk == VK_WEAK) ? dim + 1 : 1;
   op->naux_used = std::min(nu, op->naux);
-  const int npre = npre_of(d->law, dim, vk), npv = npv_stride_of(d->law, dim, vk);
+  // launch shape: E elements per CTA, ~256 threads (>= 1 element); the
+  // autotuner (atb_op_autotune) may pick another E
+  op->npre = npre_of(d->law, dim, vk);
+  op->npv = npv_stride_of(d->law, dim, vk);
   op->E = std::max(1, 256 / Np);
-  while (op->E > 1 &&
-         tend_smem_bytes(op->ns, npre, op->naux_used, dim, Nq, Np, op->Nfp, op->E, npv) > 100 * 1024)
-    --op->E;
-  op->smem = tend_smem_bytes(op->ns, npre, op->naux_used, dim, Nq, Np, op->Nfp, op->E, npv);
+  while (op->E > 1 && op_smem(op, op->E) > 100 * 1024) --op->E;
+  op->smem = op_smem(op, op->E);
   if (op->smem > 227 * 1024) {
     delete op;
     return fail(ATB_ERR_INVALID, "element too large for shared memory (%zu bytes)", op->smem);
@@ -452,12 +518,72 @@ extern "C" int atb_op_create(const atb_op_desc* d, const double* aux_host, atb_o
   cudaError_t e4 = cudaMemcpy(op->d_w, op->w.data(), Nq * sizeof(double), cudaMemcpyHostToDevice);
   cudaError_t e5 = cudaMemcpy(op->d_J, J.data(), K * sizeof(double), cudaMemcpyHostToDevice);
   cudaError_t e6 = cudaSuccess;
-  if (op->naux) e6 = cudaMemcpy(op->d_aux, aux_host, (size_t)op->naux * K * Np * sizeof(double), cudaMemcpyHostToDevice);
+  // aux: component-major over the concatenated elements
+  for (int k = 0; k < op->naux && e6 == cudaSuccess; ++k)
+    for (int inst = 0; inst < n && e6 == cudaSuccess; ++inst) {
+      const size_t Ki = (size_t)(offs[inst + 1] - offs[inst]);
+      e6 = cudaMemcpy(op->d_aux + (size_t)k * K * Np + (size_t)offs[inst] * Np, aux_hosts[inst] + (size_t)k * Ki * Np,
+                      Ki * Np * sizeof(double), cudaMemcpyHostToDevice);
+    }
   if (e1 || e2 || e3 || e4 || e5 || e6) {
     atb_op_destroy(op);
     return fail(ATB_ERR_CUDA, "uploading operator tables failed");
   }
   *out = op;
+  return ATB_OK;
+}
+
+}  // namespace
+
+extern "C" int atb_op_create(const atb_op_desc* d, const double* aux_host, atb_op** out) {
+  const double* aux[1] = {aux_host};
+  return op_create_impl(d, 1, aux, out);
+}
+
+extern "C" int atb_op_create_batch(const atb_op_desc* descs, int n, const double* const* aux_hosts, atb_op** out) {
+  return op_create_impl(descs, n, aux_hosts, out);
+}
+
+extern "C" int atb_op_autotune(atb_op* op, const double* const* q, double* scratch, void* stream, int* chosen) {
+  // times one application per candidate E (elements per CTA) and keeps the
+  // fastest; results do not depend on E (each node's arithmetic is the same)
+  if (!op || !q || !scratch) return fail(ATB_ERR_INVALID, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  double* out[5];
+  for (int s = 0; s < 5; ++s) out[s] = scratch + (size_t)(s < op->ns ? s : 0) * op->stride();
+  const int E0 = op->E;
+  int best = E0;
+  float best_ms = 1e30f;
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  for (int E = 1; E * op->Np <= 512 && E <= 16; ++E) {
+    if (op_smem(op, E) > 200 * 1024) break;
+    op->E = E;
+    op->smem = op_smem(op, E);
+    int rc = run_tendency(op, EPI_SET, q, out, nullptr, 0, 0, st);  // warm-up
+    if (rc) { op->E = E0; op->smem = op_smem(op, E0); cudaEventDestroy(a); cudaEventDestroy(b); return rc; }
+    CK(cudaEventRecord(a, st));
+    for (int r = 0; r < 5; ++r) run_tendency(op, EPI_SET, q, out, nullptr, 0, 0, st);
+    CK(cudaEventRecord(b, st));
+    CK(cudaEventSynchronize(b));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    if (ms < best_ms) { best_ms = ms; best = E; }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  op->E = best;
+  op->smem = op_smem(op, best);
+  if (chosen) *chosen = best;
+  return check_launch("autotune");
+}
+
+extern "C" int atb_op_set_launch(atb_op* op, int elements_per_cta) {
+  if (!op || elements_per_cta < 1 || elements_per_cta * op->Np > 512 || op_smem(op, elements_per_cta) > 227 * 1024)
+    return fail(ATB_ERR_INVALID, "bad elements per CTA");
+  op->E = elements_per_cta;
+  op->smem = op_smem(op, elements_per_cta);
   return ATB_OK;
 }
 
@@ -573,6 +699,10 @@ struct atb_solver {
   double* band = nullptr;
   double* blk = nullptr;
   int ld = 0;
+  // per-element time steps (LSRK over packed instances), or null; owned by
+  // the solver (atb_solver_set_instance_dt) or by the caller
+  double* d_dte = nullptr;
+  bool own_dte = false;
 };
 
 namespace {
@@ -587,6 +717,7 @@ void solver_free(atb_solver* s) {
   cudaFree(s->d_e0);
   cudaFree(s->band);
   cudaFree(s->blk);
+  if (s->own_dte) cudaFree(s->d_dte);
   delete s;
 }
 
@@ -633,6 +764,8 @@ int build_band(atb_solver* s, cudaStream_t st) {
   M.ns = ns;
   M.Np = L->Np;
   M.nh = L->Np / Nq;
+  if (!L->cols_uniform)
+    return fail(ATB_ERR_INVALID, "packed instances of an implicit operator must share their element counts");
   M.KV = L->Kd[dim - 1];
   M.KH = L->K / M.KV;
   M.nlines = M.KH * M.nh;
@@ -643,14 +776,11 @@ int build_band(atb_solver* s, cudaStream_t st) {
   if (M.bw >= 64) return fail(ATB_ERR_INVALID, "banded bandwidth too large");
   // element index of the bottom element of each horizontal stack
   std::vector<int> e0(M.nlines);
-  for (int eh = 0; eh < M.KH; ++eh) {
-    int idx[3] = {0, 0, 0}, r = eh;
-    for (int d = 0; d < dim - 1; ++d) { idx[d] = r % L->Kd[d]; r /= L->Kd[d]; }
-    idx[dim - 1] = 0;
-    int eb = L->elem_of(idx);
-    for (int hn = 0; hn < M.nh; ++hn) e0[eh * M.nh + hn] = eb;
-  }
-  M.estep = L->stacked ? 1 : M.KH;
+  for (int eh = 0; eh < M.KH; ++eh)
+    for (int hn = 0; hn < M.nh; ++hn) e0[eh * M.nh + hn] = L->col_e0[eh];
+  // vertical neighbours: next element in a stacked instance, next layer
+  // (the instance's horizontal count) otherwise
+  M.estep = L->stacked ? 1 : M.KH / L->ninst;
   int rc;
   if ((rc = dalloc(&s->d_e0, (size_t)M.nlines))) return rc;
   CK(cudaMemcpy(s->d_e0, e0.data(), e0.size() * sizeof(int), cudaMemcpyHostToDevice));
@@ -718,7 +848,8 @@ int lsrk_steps(atb_solver* s, double* const* q, int nsteps, cudaStream_t st) {
   bool in_user = true;
   for (int n = 0; n < nsteps; ++n) {
     for (size_t st_ = 0; st_ < s->rka.size(); ++st_) {
-      int rc = run_tendency(op, EPI_LSRK, cur, dq, oth, s->rka[st_], s->rkb[st_] * s->dt, st);
+      int rc = s->d_dte ? run_tendency(op, EPI_LSRK, cur, dq, oth, s->rka[st_], s->rkb[st_], st, s->d_dte)
+                        : run_tendency(op, EPI_LSRK, cur, dq, oth, s->rka[st_], s->rkb[st_] * s->dt, st);
       if (rc) return rc;
       for (int k = 0; k < 5; ++k) std::swap(cur[k], oth[k]);
       in_user = !in_user;
@@ -1042,6 +1173,79 @@ extern "C" int atb_solver_set_dt(atb_solver* s, double dt) {
   if (s->kind == ATB_ARK23 && s->lin && dt != s->dt)
     return fail(ATB_ERR_INVALID, "ARK23 factors I - dt a L for a fixed dt");
   s->dt = dt;
+  return ATB_OK;
+}
+
+extern "C" int atb_solver_set_instance_dt(atb_solver* s, const double* dt_host) {
+  if (!s) return fail(ATB_ERR_INVALID, "null solver");
+  if (s->kind != ATB_LSRK54 && s->kind != ATB_LSRK144)
+    return fail(ATB_ERR_INVALID, "per-instance time steps exist for the LSRK solvers");
+  if (!dt_host) {
+    if (s->own_dte) cudaFree(s->d_dte);
+    s->d_dte = nullptr;
+    s->own_dte = false;
+    return ATB_OK;
+  }
+  atb_op* op = s->rhs;
+  for (int i = 0; i < op->ninst; ++i)
+    if (!(dt_host[i] >= 0) || !std::isfinite(dt_host[i]))
+      return fail(ATB_ERR_INVALID, "time step of instance %d must be finite and >= 0", i);
+  std::vector<double> dte((size_t)op->K);
+  for (int i = 0; i < op->ninst; ++i)
+    for (int e = op->inst_off[i]; e < op->inst_off[i + 1]; ++e) dte[e] = dt_host[i];
+  int rc;
+  if (!s->own_dte) s->d_dte = nullptr;
+  if (!s->d_dte && (rc = dalloc(&s->d_dte, (size_t)op->K))) return rc;
+  s->own_dte = true;
+  CK(cudaMemcpy(s->d_dte, dte.data(), dte.size() * sizeof(double), cudaMemcpyHostToDevice));
+  return ATB_OK;
+}
+
+extern "C" int atb_solver_set_element_dt(atb_solver* s, const double* dte_device) {
+  if (!s) return fail(ATB_ERR_INVALID, "null solver");
+  if (s->kind != ATB_LSRK54 && s->kind != ATB_LSRK144)
+    return fail(ATB_ERR_INVALID, "per-element time steps exist for the LSRK solvers");
+  if (s->d_dte && s->own_dte) cudaFree(s->d_dte);
+  s->d_dte = const_cast<double*>(dte_device);
+  s->own_dte = false;
+  return ATB_OK;
+}
+
+extern "C" int atb_op_set_active(atb_op* op, int n_instances) {
+  if (!op || n_instances < 0 || n_instances > op->ninst) return fail(ATB_ERR_INVALID, "bad active instance count");
+  op->K_active = op->inst_off[n_instances];
+  return ATB_OK;
+}
+
+extern "C" int atb_op_set_instance_aux(atb_op* op, int i, const double* aux_host, void* stream) {
+  if (!op || i < 0 || i >= op->ninst) return fail(ATB_ERR_INVALID, "bad instance");
+  if (op->naux == 0) return ATB_OK;
+  if (!aux_host) return fail(ATB_ERR_INVALID, "aux fields missing");
+  const size_t Ki = (size_t)(op->inst_off[i + 1] - op->inst_off[i]), n = Ki * op->Np;
+  for (int k = 0; k < op->naux; ++k)
+    CK(cudaMemcpyAsync(op->d_aux + (size_t)k * op->stride() + (size_t)op->inst_off[i] * op->Np, aux_host + k * n,
+                       n * sizeof(double), cudaMemcpyHostToDevice, (cudaStream_t)stream));
+  return ATB_OK;
+}
+
+extern "C" int atb_op_copy_instance_aux(atb_op* op, int dst, int src, void* stream) {
+  if (!op || dst < 0 || src < 0 || dst >= op->ninst || src >= op->ninst) return fail(ATB_ERR_INVALID, "bad instance");
+  const int Kd = op->inst_off[dst + 1] - op->inst_off[dst], Ks = op->inst_off[src + 1] - op->inst_off[src];
+  if (Kd != Ks) return fail(ATB_ERR_INVALID, "instances %d and %d differ in size", dst, src);
+  if (dst == src || op->naux == 0) return ATB_OK;
+  const size_t n = (size_t)Kd * op->Np;
+  for (int k = 0; k < op->naux; ++k)
+    CK(cudaMemcpyAsync(op->d_aux + (size_t)k * op->stride() + (size_t)op->inst_off[dst] * op->Np,
+                       op->d_aux + (size_t)k * op->stride() + (size_t)op->inst_off[src] * op->Np, n * sizeof(double),
+                       cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  return ATB_OK;
+}
+
+extern "C" int atb_op_instances(const atb_op* op, int* n, int* first_elements) {
+  if (!op || !n) return fail(ATB_ERR_INVALID, "null argument");
+  *n = op->ninst;
+  if (first_elements)
+    for (int i = 0; i <= op->ninst; ++i) first_elements[i] = op->inst_off[i];
   return ATB_OK;
 }
 

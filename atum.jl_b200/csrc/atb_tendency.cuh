@@ -27,8 +27,9 @@
 // Epilogues (runtime-uniform):
 //   EPI_SET      out = T                         (increment = false)
 //   EPI_ADD      out += T                        (increment = true)
-//   EPI_LSRK     out = a*out + T; out2 = q + bdt*out   (2N-storage LSRK stage,
-//                                                 out2 is a second state buffer)
+//   EPI_LSRK     out = a*out + T; out2 = q + bdt*out   (2N-storage LSRK stage;
+//                out2 is a second state buffer; with dte set, bdt*dte[e]
+//                replaces bdt, so each packed instance takes its own step)
 //   EPI_SUBOUT2  out = T; out2 -= T              (ARK, split_rhs = false:
 //                                                 im_K = L(Q), ex_K -= im_K)
 //   EPI_RLSRK    out = T; out2 = a*out2 + T      (relaxation LSRK: k, dq)
@@ -51,7 +52,8 @@ struct TendArgs {
   LawP law;
   int dirs, sflux, epi;
   double a, bdt;
-  size_t stride;  // K*Np
+  const double* dte;  // per-element time step (batched instances), or null
+  size_t stride;      // K*Np
   const double* q[5];
   double* out[5];
   double* out2[5];
@@ -567,14 +569,15 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
 #pragma unroll
       for (int s = 0; s < NS; ++s) A.out[s][gid] = A.out[s][gid] + T[s];
       break;
-    case EPI_LSRK:
+    case EPI_LSRK: {
+      const double bdt = A.dte ? A.bdt * A.dte[e] : A.bdt;
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
         const double dqn = A.a * A.out[s][gid] + T[s];
         A.out[s][gid] = dqn;
-        A.out2[s][gid] = qn[s] + A.bdt * dqn;
+        A.out2[s][gid] = qn[s] + bdt * dqn;
       }
-      break;
+    } break;
     case EPI_SUBOUT2:
 #pragma unroll
       for (int s = 0; s < NS; ++s) {

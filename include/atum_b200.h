@@ -107,6 +107,36 @@ int atb_op_create(const atb_op_desc* desc, const double* aux_host, atb_op** out)
 int atb_op_destroy(atb_op* op);
 int atb_op_dims(const atb_op* op, int* ns, int* K, int* Np);
 
+/* Multi-instance batching (no reference counterpart; the reference builds one
+ * DGSEM per problem, src/dgsem.jl:38-56, and steps each alone).  n instances
+ * that share law, order, forms, fluxes, directions, precision, constants and
+ * problem kinds -- grids may differ -- become one operator whose elements are
+ * the instances' elements concatenated (instance i owns elements
+ * [first_i, first_{i+1})); neighbour indices stay inside each instance, so
+ * every instance's result is bitwise the one it gets alone.  Fields of the
+ * packed operator are the instances' fields concatenated per component.
+ * aux_hosts[i]: instance i's aux fields (naux*K_i*Np, component-major). */
+int atb_op_create_batch(const atb_op_desc* descs, int n, const double* const* aux_hosts, atb_op** out);
+/* instance count and the n+1 element offsets (first_elements may be NULL) */
+int atb_op_instances(const atb_op* op, int* n, int* first_elements);
+/* Serving support (no reference counterpart).  atb_op_set_active limits
+ * tendency launches to the first n instances (elements [0, first_n)); the
+ * others keep their state untouched by applications of the operator.  It
+ * changes a host-side launch parameter, so a captured CUDA graph keeps the
+ * value it was captured with.  atb_op_set_instance_aux replaces instance i's
+ * aux fields (naux*K_i*Np host doubles, component-major) with copies ordered on
+ * `stream`; atb_op_copy_instance_aux copies instance src's aux fields over
+ * instance dst's (equal sizes) on `stream`. */
+int atb_op_set_active(atb_op* op, int n_instances);
+int atb_op_set_instance_aux(atb_op* op, int i, const double* aux_host, void* stream);
+int atb_op_copy_instance_aux(atb_op* op, int dst, int src, void* stream);
+/* Launch-shape tuning (no reference counterpart): times the tendency kernel
+ * for every admissible elements-per-CTA count on state q (scratch: ns*K*Np
+ * doubles of device memory, overwritten) and keeps the fastest; *chosen gets
+ * it.  Results do not depend on the shape.  atb_op_set_launch sets it. */
+int atb_op_autotune(atb_op* op, const double* const* q, double* scratch, void* stream, int* chosen);
+int atb_op_set_launch(atb_op* op, int elements_per_cta);
+
 /* (dg::DGSEM)(dq, q, time; increment) -- src/dgsem.jl:59-98 */
 int atb_op_apply(atb_op* op, double* const* dq, const double* const* q, double time, int increment, void* stream);
 
@@ -123,6 +153,16 @@ int atb_solver_step(atb_solver* s, double* const* q, int nsteps, void* stream);
 int atb_solve(atb_solver* s, double* const* q, double timeend, int adjust_final, int* steps_out, void* stream);
 int atb_solver_get(const atb_solver* s, double* time, double* dt, double* gamma);
 int atb_solver_set_dt(atb_solver* s, double dt);
+/* Per-instance time steps for an LSRK solver over a packed operator (no
+ * reference counterpart): dt_host holds one step per instance (host memory,
+ * copied synchronously; 0 freezes an instance); NULL returns to the solver's
+ * single dt.  The solver's own clock still advances by its dt; per-instance
+ * times are the caller's bookkeeping.  atb_solver_set_element_dt instead hands
+ * the solver a caller-owned device array of one time step per element (K
+ * doubles), read by every later stage, so its contents may change between
+ * steps without another call; NULL returns to the single dt. */
+int atb_solver_set_instance_dt(atb_solver* s, const double* dt_host);
+int atb_solver_set_element_dt(atb_solver* s, const double* dte_device);
 
 /* measures -- src/measures.jl:6-33 (p = 2 or INFINITY); results to host memory */
 int atb_weightednorm(atb_op* op, const double* const* q, double p, double* comp_host, double* total_host,
