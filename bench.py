@@ -327,7 +327,10 @@ def run_ours(args):
                      "achieved": tflops, "peak": peak_fp64.value, "unit": "TFLOP/s",
                      "frac": tflops / peak_fp64.value if peak_fp64.value > 0 else None,
                      "peak_source": "measured in this run: FP64 FMA probe (atb_probe_fp64_peak)",
-                     "flops_per_launch": flops_launch, "avg_launch_ms": avg_ms, "traffic": None,
+                     "flops_per_launch": flops_launch, "avg_launch_ms": avg_ms,
+                     "traffic": profiled_traffic() if args.precision == "fp64" else None,
+                     "traffic_unit": "bytes per launch (dram read + write, one ncu capture)",
+                     "traffic_source": PROFILE_TEND,
                      "hbm_view": {"bytes_per_launch": bytes_launch,
                                   "achieved_gbs": bytes_launch / (avg_ms * 1e-3) / 1e9,
                                   "peak_gbs": peaks["hbm_gbs"], "peak_kind": kind}},
@@ -340,6 +343,23 @@ def run_ours(args):
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+PROFILE_TEND = "profiles/tendency_eg3_ec_nq5_bubble16.md"
+
+
+def profiled_traffic():
+    """DRAM bytes (read + write) of one FP64 tendency launch of this workload,
+    from the committed ncu summary of the same kernel and workload."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), PROFILE_TEND)
+    try:
+        with open(path) as f:
+            for ln in f:
+                if ln.startswith("traffic_bytes_per_launch:"):
+                    return int(ln.split(":")[1])
+    except OSError:
+        pass
+    return None
 
 
 def main():
