@@ -55,6 +55,9 @@ SIGNATURES = {
     "atb_op_autotune": [_VP, PtrArr, _DP, _VP, _IP],
     "atb_op_set_launch": [_VP, C.c_int],
     "atb_op_set_active": [_VP, C.c_int],
+    "atb_op_create_pool": [C.POINTER(OpDesc), C.c_int, C.POINTER(C.c_void_p)],
+    "atb_op_place_instance": [_VP, C.c_int, C.POINTER(OpDesc), _DP, _VP],
+    "atb_op_set_active_elements": [_VP, C.c_int],
     "atb_op_set_instance_aux": [_VP, C.c_int, _DP, _VP],
     "atb_op_copy_instance_aux": [_VP, C.c_int, C.c_int, _VP],
     "atb_op_apply": [_VP, PtrArr, PtrArr, C.c_double, C.c_int, _VP],

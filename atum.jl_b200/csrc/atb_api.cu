@@ -137,6 +137,7 @@ struct atb_op {
   int dim = 0, N = 0, Nq = 0, Np = 0, Nfp = 0, K = 0, Kd[3] = {1, 1, 1}, ns = 0, naux = 0;
   int vk = 0, dirs = 0, sflux = 0, precision = 0, stacked = 0;
   int naux_used = 0;  // leading aux components the tendency kernel stages
+  atb_op_desc kind{};  // instance 0's descriptor (kind checks of later placements)
   int ninst = 1;      // instances packed into this operator
   int K_active = 0;   // elements the tendency launches cover (a prefix of K)
   std::vector<int> inst_off;  // first element of each instance, then K
@@ -302,6 +303,59 @@ bool same_kind(const atb_op_desc* a, const atb_op_desc* b) {
   return ok;
 }
 
+// Geometry of one instance whose elements start at `off` in the packed
+// ordering: 2/h per dimension, Jacobian determinant, neighbour table
+// (absolute element, or -(face number) on a non-periodic boundary), and the
+// bottom element of every vertical column.  Outputs hold the instance's own
+// elements only (element off + e at index e).
+int instance_geometry(const atb_op_desc* di, int off, double* ginv, double* J, int* nbr, std::vector<int>* col_e0) {
+  const int dim = di->dim;
+  int Kd[3] = {1, 1, 1};
+  for (int k = 0; k < dim; ++k) Kd[k] = di->K[k];
+  if (col_e0) {
+    // vertical columns (last dimension), horizontal element index fastest
+    int KH = 1;
+    for (int k = 0; k < dim - 1; ++k) KH *= Kd[k];
+    for (int eh = 0; eh < KH; ++eh) {
+      int ci[3] = {0, 0, 0}, r = eh;
+      for (int k = 0; k < dim - 1; ++k) { ci[k] = r % Kd[k]; r /= Kd[k]; }
+      col_e0->push_back(off + elem_index(di, ci));
+    }
+  }
+  int idx[3];
+  for (idx[2] = 0; idx[2] < Kd[2]; ++idx[2])
+    for (idx[1] = 0; idx[1] < Kd[1]; ++idx[1])
+      for (idx[0] = 0; idx[0] < Kd[0]; ++idx[0]) {
+        const int e = elem_index(di, idx);
+        double Je = 1.0;
+        for (int k = 0; k < 3; ++k) ginv[e * 3 + k] = 0.0;
+        for (int k = 0; k < dim; ++k) {
+          const double h = di->vertices[k][idx[k] + 1] - di->vertices[k][idx[k]];
+          if (!(h > 0)) return ATB_ERR_INVALID;
+          ginv[e * 3 + k] = 2.0 / h;
+          Je *= h / 2;
+        }
+        J[e] = Je;
+        for (int k = 0; k < 3; ++k)
+          for (int f = 0; f < 2; ++f) {
+            const int face = 2 * k + f;
+            if (k >= dim) { nbr[e * 6 + face] = -(face + 1); continue; }
+            int nb[3] = {idx[0], idx[1], idx[2]};
+            nb[k] += f ? 1 : -1;
+            if (nb[k] < 0 || nb[k] >= Kd[k]) {
+              if (di->periodic[k]) {
+                nb[k] = (nb[k] + Kd[k]) % Kd[k];
+              } else {
+                nbr[e * 6 + face] = -(face + 1);  // boundary tag = face number
+                continue;
+              }
+            }
+            nbr[e * 6 + face] = off + elem_index(di, nb);
+          }
+      }
+  return ATB_OK;
+}
+
 // One operator over n instances that share their law, order, fluxes,
 // precision and problem kinds: their elements are concatenated (instance i
 // owns elements [off_i, off_i + K_i)) and every neighbour index is offset, so
@@ -388,6 +442,7 @@ int op_create_impl(const atb_op_desc* descs, int n, const double* const* aux_hos
   }
   op->K = offs[n];
   op->K_active = op->K;
+  op->kind = *d;
   op->inst_off = offs;
   for (int k = 0; k < 3; ++k) op->Kd[k] = k < d->dim ? d->K[k] : 1;  // instance 0
   for (int i = 1; i < n; ++i)
@@ -430,53 +485,12 @@ int op_create_impl(const atb_op_desc* descs, int n, const double* const* aux_hos
   std::vector<double> ginv((size_t)K * 3, 0.0), J(K, 1.0);
   std::vector<int> nbr((size_t)K * 6, 0);
   for (int inst = 0; inst < n; ++inst) {
-    const atb_op_desc* di = &descs[inst];
-    const int off = offs[inst];
-    int Kd[3] = {1, 1, 1};
-    for (int k = 0; k < dim; ++k) Kd[k] = di->K[k];
-    int idx[3];
-    {
-      // vertical columns (last dimension), horizontal element index fastest
-      int KH = 1;
-      for (int k = 0; k < dim - 1; ++k) KH *= Kd[k];
-      for (int eh = 0; eh < KH; ++eh) {
-        int ci[3] = {0, 0, 0}, r = eh;
-        for (int k = 0; k < dim - 1; ++k) { ci[k] = r % Kd[k]; r /= Kd[k]; }
-        op->col_e0.push_back(off + elem_index(di, ci));
-      }
+    const int rc = instance_geometry(&descs[inst], offs[inst], ginv.data() + (size_t)offs[inst] * 3,
+                                     J.data() + offs[inst], nbr.data() + (size_t)offs[inst] * 6, &op->col_e0);
+    if (rc) {
+      delete op;
+      return fail(rc, "vertex vectors of instance %d are not increasing", inst);
     }
-    for (idx[2] = 0; idx[2] < Kd[2]; ++idx[2])
-      for (idx[1] = 0; idx[1] < Kd[1]; ++idx[1])
-        for (idx[0] = 0; idx[0] < Kd[0]; ++idx[0]) {
-          const int e = off + elem_index(di, idx);
-          double Je = 1.0;
-          for (int k = 0; k < dim; ++k) {
-            const double h = di->vertices[k][idx[k] + 1] - di->vertices[k][idx[k]];
-            if (!(h > 0)) {
-              delete op;
-              return fail(ATB_ERR_INVALID, "vertex vector %d of instance %d is not increasing", k, inst);
-            }
-            ginv[e * 3 + k] = 2.0 / h;
-            Je *= h / 2;
-          }
-          J[e] = Je;
-          for (int k = 0; k < 3; ++k)
-            for (int f = 0; f < 2; ++f) {
-              int face = 2 * k + f;
-              if (k >= dim) { nbr[e * 6 + face] = -(face + 1); continue; }
-              int nb[3] = {idx[0], idx[1], idx[2]};
-              nb[k] += f ? 1 : -1;
-              if (nb[k] < 0 || nb[k] >= Kd[k]) {
-                if (di->periodic[k]) {
-                  nb[k] = (nb[k] + Kd[k]) % Kd[k];
-                } else {
-                  nbr[e * 6 + face] = -(face + 1);  // boundary tag = face number
-                  continue;
-                }
-              }
-              nbr[e * 6 + face] = off + elem_index(di, nb);
-            }
-        }
   }
   // aux components the kernels read: Euler-gravity needs Phi (fluxes, wave
   // speeds), grad Phi for the weak form's non-conservative term, and the
@@ -542,6 +556,70 @@ extern "C" int atb_op_create(const atb_op_desc* d, const double* aux_host, atb_o
 
 extern "C" int atb_op_create_batch(const atb_op_desc* descs, int n, const double* const* aux_hosts, atb_op** out) {
   return op_create_impl(descs, n, aux_hosts, out);
+}
+
+extern "C" int atb_op_create_pool(const atb_op_desc* kind, int capacity_elements, atb_op** out) {
+  if (!kind || !out) return fail(ATB_ERR_INVALID, "null argument");
+  if (capacity_elements < 1) return fail(ATB_ERR_INVALID, "capacity must be >= 1 element");
+  // placeholder geometry: one row of unit elements along the first dimension
+  atb_op_desc d = *kind;
+  std::vector<double> v((size_t)capacity_elements + 1), u(2);
+  for (int i = 0; i <= capacity_elements; ++i) v[i] = i;
+  u[0] = 0;
+  u[1] = 1;
+  d.K[0] = capacity_elements;
+  d.vertices[0] = v.data();
+  for (int k = 1; k < 3; ++k) { d.K[k] = 1; d.vertices[k] = u.data(); }
+  d.stacked = 0;
+  int Np = 1;
+  for (int k = 0; k < d.dim; ++k) Np *= d.N + 1;
+  std::vector<double> aux((size_t)std::max(0, d.naux) * capacity_elements * Np, 0.0);
+  const double* auxp[1] = {aux.data()};
+  const int rc = op_create_impl(&d, 1, auxp, out);
+  if (rc) return rc;
+  (*out)->K_active = 0;
+  (*out)->col_e0.clear();
+  (*out)->cols_uniform = false;  // placements have their own grids: no banded solve
+  return ATB_OK;
+}
+
+extern "C" int atb_op_place_instance(atb_op* op, int first_element, const atb_op_desc* desc, const double* aux_host,
+                                     void* stream) {
+  if (!op || !desc) return fail(ATB_ERR_INVALID, "null argument");
+  if (!same_kind(&op->kind, desc))
+    return fail(ATB_ERR_INVALID, "placed instance differs from the pool in law, order, fluxes, precision or "
+                                 "problem kinds");
+  int Ki = 1;
+  for (int k = 0; k < desc->dim; ++k) {
+    if (desc->K[k] < 1 || !desc->vertices[k]) return fail(ATB_ERR_INVALID, "bad grid of placed instance");
+    Ki *= desc->K[k];
+  }
+  if (first_element < 0 || (long)first_element + Ki > op->K)
+    return fail(ATB_ERR_INVALID, "placement [%d, %ld) outside the pool's %d elements", first_element,
+                (long)first_element + Ki, op->K);
+  if (op->naux > 0 && !aux_host) return fail(ATB_ERR_INVALID, "aux fields missing");
+  std::vector<double> ginv((size_t)Ki * 3), J(Ki);
+  std::vector<int> nbr((size_t)Ki * 6);
+  if (instance_geometry(desc, first_element, ginv.data(), J.data(), nbr.data(), nullptr))
+    return fail(ATB_ERR_INVALID, "vertex vectors of the placed instance are not increasing");
+  cudaStream_t st = (cudaStream_t)stream;
+  // pageable-source async copies: the sources may be released on return
+  CK(cudaMemcpyAsync(op->d_ginv + (size_t)first_element * 3, ginv.data(), ginv.size() * sizeof(double),
+                     cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(op->d_J + first_element, J.data(), J.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(op->d_nbr + (size_t)first_element * 6, nbr.data(), nbr.size() * sizeof(int),
+                     cudaMemcpyHostToDevice, st));
+  const size_t n = (size_t)Ki * op->Np;
+  for (int k = 0; k < op->naux; ++k)
+    CK(cudaMemcpyAsync(op->d_aux + (size_t)k * op->stride() + (size_t)first_element * op->Np, aux_host + k * n,
+                       n * sizeof(double), cudaMemcpyHostToDevice, st));
+  return ATB_OK;
+}
+
+extern "C" int atb_op_set_active_elements(atb_op* op, int n_elements) {
+  if (!op || n_elements < 0 || n_elements > op->K) return fail(ATB_ERR_INVALID, "bad active element count");
+  op->K_active = n_elements;
+  return ATB_OK;
 }
 
 extern "C" int atb_op_autotune(atb_op* op, const double* const* q, double* scratch, void* stream, int* chosen) {

@@ -27,9 +27,9 @@
 // Epilogues (runtime-uniform):
 //   EPI_SET      out = T                         (increment = false)
 //   EPI_ADD      out += T                        (increment = true)
-//   EPI_LSRK     out = a*out + T; out2 = q + bdt*out   (2N-storage LSRK stage;
-//                out2 is a second state buffer; with dte set, bdt*dte[e]
-//                replaces bdt, so each packed instance takes its own step)
+//   EPI_LSRK     out = a*out + T (out = T when a = 0); out2 = q + bdt*out
+//                (2N-storage LSRK stage, out2 a second state buffer; with
+//                dte set, bdt*dte[e] replaces bdt: per-instance steps)
 //   EPI_SUBOUT2  out = T; out2 -= T              (ARK, split_rhs = false:
 //                                                 im_K = L(Q), ex_K -= im_K)
 //   EPI_RLSRK    out = T; out2 = a*out2 + T      (relaxation LSRK: k, dq)
@@ -573,7 +573,9 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
       const double bdt = A.dte ? A.bdt * A.dte[e] : A.bdt;
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
-        const double dqn = A.a * A.out[s][gid] + T[s];
+        // first stage (a = 0): the previous increment is not read, so stale
+        // or never-written increment storage cannot leak into the step
+        const double dqn = (A.a != 0.0) ? A.a * A.out[s][gid] + T[s] : T[s];
         A.out[s][gid] = dqn;
         A.out2[s][gid] = qn[s] + bdt * dqn;
       }

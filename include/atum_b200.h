@@ -128,6 +128,20 @@ int atb_op_instances(const atb_op* op, int* n, int* first_elements);
  * `stream`; atb_op_copy_instance_aux copies instance src's aux fields over
  * instance dst's (equal sizes) on `stream`. */
 int atb_op_set_active(atb_op* op, int n_instances);
+/* Element pools for serving (no reference counterpart).  atb_op_create_pool
+ * makes an operator of `kind` (law, order, forms, fluxes, precision, problem
+ * kinds and constants of the descriptor; its grid is ignored) with room for
+ * capacity_elements elements and none active.  atb_op_place_instance writes
+ * the geometry (metrics, neighbour table offset by first_element) and aux
+ * fields of the instance `desc` (same kind, any grid) into elements
+ * [first_element, first_element + K) with copies ordered on `stream`; host
+ * sources may be released on return.  atb_op_set_active_elements sets how
+ * many leading elements tendency launches cover; a caller keeps its placed
+ * instances inside that prefix.  Pools have no banded solve (ARK23). */
+int atb_op_create_pool(const atb_op_desc* kind, int capacity_elements, atb_op** out);
+int atb_op_place_instance(atb_op* op, int first_element, const atb_op_desc* desc, const double* aux_host,
+                          void* stream);
+int atb_op_set_active_elements(atb_op* op, int n_elements);
 int atb_op_set_instance_aux(atb_op* op, int i, const double* aux_host, void* stream);
 int atb_op_copy_instance_aux(atb_op* op, int dst, int src, void* stream);
 /* Launch-shape tuning (no reference counterpart): times the tendency kernel
