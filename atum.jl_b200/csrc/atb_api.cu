@@ -361,7 +361,8 @@ int instance_geometry(const atb_op_desc* di, int off, double* ginv, double* J, i
 // owns elements [off_i, off_i + K_i)) and every neighbour index is offset, so
 // the tendency kernel -- which only sees an element list -- advances all of
 // them in one launch (the instances never couple).
-int op_create_impl(const atb_op_desc* descs, int n, const double* const* aux_hosts, atb_op** out) {
+int op_create_impl(const atb_op_desc* descs, int n, const double* const* aux_hosts, atb_op** out,
+                   bool zero_aux = false) {
   if (!descs || !out || n < 1) return fail(ATB_ERR_INVALID, "null argument");
   *out = nullptr;
   const atb_op_desc* d = &descs[0];
@@ -378,7 +379,8 @@ int op_create_impl(const atb_op_desc* descs, int n, const double* const* aux_hos
     if (i > 0 && !same_kind(d, &descs[i]))
       return fail(ATB_ERR_INVALID, "batched instance %d differs from instance 0 in law, order, fluxes, "
                                    "precision or problem kinds", i);
-    if (descs[i].naux > 0 && (!aux_hosts || !aux_hosts[i])) return fail(ATB_ERR_INVALID, "aux fields missing");
+    if (descs[i].naux > 0 && !zero_aux && (!aux_hosts || !aux_hosts[i]))
+      return fail(ATB_ERR_INVALID, "aux fields missing");
     for (int k = 0; k < d->dim; ++k) {
       if (descs[i].K[k] < 1) return fail(ATB_ERR_INVALID, "K[%d] must be >= 1", k);
       if (!descs[i].vertices[k]) return fail(ATB_ERR_INVALID, "vertex vector %d missing", k);
@@ -533,7 +535,8 @@ int op_create_impl(const atb_op_desc* descs, int n, const double* const* aux_hos
   cudaError_t e5 = cudaMemcpy(op->d_J, J.data(), K * sizeof(double), cudaMemcpyHostToDevice);
   cudaError_t e6 = cudaSuccess;
   // aux: component-major over the concatenated elements
-  for (int k = 0; k < op->naux && e6 == cudaSuccess; ++k)
+  if (zero_aux) e6 = cudaMemset(op->d_aux, 0, (size_t)std::max(1, op->naux) * K * Np * sizeof(double));
+  for (int k = 0; k < op->naux && e6 == cudaSuccess && !zero_aux; ++k)
     for (int inst = 0; inst < n && e6 == cudaSuccess; ++inst) {
       const size_t Ki = (size_t)(offs[inst + 1] - offs[inst]);
       e6 = cudaMemcpy(op->d_aux + (size_t)k * K * Np + (size_t)offs[inst] * Np, aux_hosts[inst] + (size_t)k * Ki * Np,
@@ -571,11 +574,7 @@ extern "C" int atb_op_create_pool(const atb_op_desc* kind, int capacity_elements
   d.vertices[0] = v.data();
   for (int k = 1; k < 3; ++k) { d.K[k] = 1; d.vertices[k] = u.data(); }
   d.stacked = 0;
-  int Np = 1;
-  for (int k = 0; k < d.dim; ++k) Np *= d.N + 1;
-  std::vector<double> aux((size_t)std::max(0, d.naux) * capacity_elements * Np, 0.0);
-  const double* auxp[1] = {aux.data()};
-  const int rc = op_create_impl(&d, 1, auxp, out);
+  const int rc = op_create_impl(&d, 1, nullptr, out, /*zero_aux=*/true);
   if (rc) return rc;
   (*out)->K_active = 0;
   (*out)->col_e0.clear();

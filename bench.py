@@ -348,6 +348,231 @@ def run_ours(args):
 PROFILE_TEND = "profiles/tendency_eg3_ec_nq5_bubble16.md"
 
 
+# ------------------------------------------------------------ serving stream
+def run_serve(args):
+    """Seeded Poisson stream of requests served by continuous batching: 2-D
+    Euler isentropic vortices (periodic [-5,5]^2, 16^2..128^2 elements) and
+    3-D Euler-gravity rising bubbles (8^3..32^3 elements), orders N uniform in
+    2..7, FP32 flux / FP64 state, LSRK54 at CFL 0.3, end times uniform in
+    0.5..5 flow-through times multiplied by --time-scale (a full flow-through
+    takes thousands of steps per request; the scale keeps the run to about a
+    minute).  Requests are admitted under an HBM budget and packed by (law, N).
+    Reports throughput, p50/p99 latency, and the relative L2 error of a sample
+    of requests against the same request stepped alone by the FP64 path."""
+    import numpy as np
+    import torch
+
+    dist, rank, world = dist_init()
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    A = load_pkg()
+    import problems as P
+
+    rng = np.random.default_rng(20261203 + rank)
+    vortex_K = list(range(16, 129, 16))
+    bubble_K = [8, 16, 24, 32]
+    cache = {}
+
+    def spec(kind, K, N, precision):
+        key = (kind, K, N, precision)
+        if key not in cache:
+            if kind == "vortex":
+                c = P.vortex_c1(N=N, K=K, precision=precision)
+                flow = 10.0 / math.sqrt(2.0)          # domain / |u|
+            else:
+                c = P.bubble_3d(N=N, K=K, imex=False, precision=precision)
+                flow = 10e3 / 340.0                   # box / sound speed
+            cache[key] = (c, flow)
+        return cache[key]
+
+    reqs = []
+    t = 0.0
+    for i in range(args.requests):
+        t += rng.exponential(1.0 / args.rate)
+        kind = "vortex" if rng.random() < 0.5 else "bubble"
+        K = int(rng.choice(vortex_K if kind == "vortex" else bubble_K))
+        N = int(rng.integers(2, 8))
+        c, flow = spec(kind, K, N, "fp32flux")
+        tend = rng.uniform(0.5, 5.0) * flow * args.time_scale
+        nsteps = max(1, int(math.ceil(tend / c.dt)))
+        reqs.append(A.serving.Request(rid=i, dg=c.dg, q0=c.q0, dt=c.dt, nsteps=nsteps, arrival=t))
+    srv = A.serving.Server(hbm_budget_bytes=args.hbm_budget_gb * 1e9, capacity=args.pool_elements,
+                           chunk=256, use_graphs=True)
+    # warm-up stream (a few requests), then the measured one
+    warm = [A.serving.Request(rid=-1 - j, dg=r.dg, q0=r.q0, dt=r.dt, nsteps=min(r.nsteps, 4), arrival=0.0)
+            for j, r in enumerate(reqs[:args.warmup])]
+    srv.run(warm, realtime=False)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        st = srv.run(reqs, realtime=True)
+    # accuracy: a sample of requests stepped alone in FP64
+    errs = []
+    for r in reqs[:: max(1, len(reqs) // args.error_samples)][: args.error_samples]:
+        kind = "vortex" if r.dg.law.dim == 2 else "bubble"
+        c64, _ = spec(kind, int(round(r.dg.grid.Kd[0])), r.dg.grid.cell.N, "fp64")
+        q = torch.as_tensor(c64.q0, device="cuda").contiguous()
+        A.LSRK54(c64.dg, q, r.dt).step(q, r.nsteps)
+        ref = q.cpu().numpy()
+        MJ = c64.dg.MJ
+        num = sum(float(np.sum(MJ * (r.result[s] - ref[s]) ** 2)) for s in range(ref.shape[0]))
+        den = sum(float(np.sum(MJ * ref[s] ** 2)) for s in range(ref.shape[0]))
+        errs.append(math.sqrt(num / den))
+    srv.close()
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+    lat = np.array([r.latency for r in reqs])
+    line = {
+        "metric": "DOF-stage updates/s", "value": st.dof_stage_per_s * world, "unit": "DOF-stage/s",
+        "n_gpus": world, "steps": int(sum(r.nsteps for r in reqs)), "warmup": args.warmup,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64-state/f32-flux", "data": "synthetic",
+        "config": {"workload": "serving: Poisson stream of 2-D Euler vortices (16^2..128^2) and 3-D Euler-gravity "
+                               "bubbles (8^3..32^3), N in 2..7, FP32 flux / FP64 state, LSRK54, packed by (law, N)",
+                   "requests": args.requests, "rate_per_s": args.rate, "time_scale": args.time_scale,
+                   "hbm_budget_gb": args.hbm_budget_gb, "pool_elements": args.pool_elements},
+        "latency_s": {"p50": st.p50_latency_s, "p99": st.p99_latency_s, "mean": st.mean_latency_s,
+                      "max": float(lat.max())},
+        "makespan_s": st.makespan_s, "pools": st.pools, "ticks": st.ticks,
+        "peak_pool_bytes": st.peak_pool_bytes, "dof_stage_updates": st.extra["dof_stage_updates"],
+        "rel_l2_vs_fp64": {"samples": len(errs), "max": max(errs) if errs else None,
+                           "median": float(np.median(errs)) if errs else None},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+# ------------------------------------------- batched shallow-water instances
+def run_swbatch(args):
+    """256 rotating shallow-water instances (f-plane, g = 9.81), each a
+    periodic 32 x 32 square of N = 4 elements with its own seeded bathymetry
+    and height perturbation, packed into one operator (atb_op_create_batch)
+    and stepped by LSRK54 with FP32 flux arithmetic and FP64 state.  Reports
+    the packed FP32-flux throughput beside the packed FP64 run and the plain
+    FP64 path (one instance at a time) on the same inputs, the relative L2
+    error and mass drift against the FP64 run, and lake-at-rest residuals."""
+    import numpy as np
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    dist, rank, world = dist_init()
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    A = load_pkg()
+    import problems as P
+
+    n_inst, K, N = args.instances, 32, 4
+    steps = args.steps if args.steps is not None else 500
+    seeds = [1000 * (rank + 1) + i for i in range(n_inst)]
+
+    def cases(precision, lake=False, n=n_inst):
+        return [P.sw_fplane(N=N, K=K, seed=sd, precision=precision, lake_at_rest=lake, steps=steps)
+                for sd in seeds[:n]]
+
+    c32, c64 = cases("fp32flux"), cases("fp64")
+    dt = min(c.dt for c in c64)
+    p32 = A.batch.PackedDGSEM([c.dg for c in c32])
+    p64 = A.batch.PackedDGSEM([c.dg for c in c64])
+    q0 = p64.pack([torch.as_tensor(c.q0, device="cuda") for c in c64])
+    dofs = q0.numel()
+    MJ = torch.as_tensor(c64[0].dg.MJ, device="cuda")  # identical grids
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def timed(packed, q, nsteps, warm):
+        s = A.LSRK54(packed, q, dt)
+        s.step(q, warm)
+        q.copy_(q0)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        s.step(q, nsteps)
+        e1.record()
+        barrier()
+        return e0.elapsed_time(e1)
+
+    E32 = p32.autotune(q0.clone())
+    E64 = p64.autotune(q0.clone())
+    q32, q64 = q0.clone(), q0.clone()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ms32 = timed(p32, q32, steps, args.warmup)
+    ms64 = timed(p64, q64, steps, args.warmup)
+    # plain FP64 path: the same instances one at a time (sample of 8)
+    nseq = min(8, n_inst)
+    qs = [torch.as_tensor(c.q0, device="cuda").contiguous() for c in c64[:nseq]]
+    sol = [A.LSRK54(c.dg, q, dt) for c, q in zip(c64[:nseq], qs)]
+    for s_, q in zip(sol, qs):
+        s_.step(q, args.warmup)
+    for c, q in zip(c64[:nseq], qs):
+        q.copy_(torch.as_tensor(c.q0, device="cuda"))
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for s_, q in zip(sol, qs):
+        s_.step(q, steps)
+    e1.record()
+    barrier()
+    ms_seq = e0.elapsed_time(e1)
+    dofs_inst = dofs // n_inst
+
+    # accuracy: per instance relative L2 (MJ-weighted) against the FP64 run
+    def per_inst(q):
+        return q.reshape(q.shape[0], n_inst, -1, q.shape[-1])
+
+    a, b = per_inst(q32), per_inst(q64)
+    w = MJ[None, None]
+    err = torch.sqrt(((a - b) ** 2 * w).sum(dim=(0, 2, 3)) / (b ** 2 * w).sum(dim=(0, 2, 3)))
+    mass0 = (per_inst(q0)[0] * MJ[None]).sum(dim=(1, 2))
+    drift32 = ((a[0] * MJ[None]).sum(dim=(1, 2)) - mass0).abs() / mass0
+    drift64 = ((b[0] * MJ[None]).sum(dim=(1, 2)) - mass0).abs() / mass0
+    # lake at rest in the FP32-flux form: surface and velocity residuals
+    nl = min(16, n_inst)
+    cl = cases("fp32flux", lake=True, n=nl)
+    pl = A.batch.PackedDGSEM([c.dg for c in cl])
+    ql = pl.pack([torch.as_tensor(c.q0, device="cuda") for c in cl])
+    bl = torch.cat([torch.as_tensor(c.dg.auxstate_host()[0], device="cuda") for c in cl], dim=0)
+    A.LSRK54(pl, ql, dt).step(ql, steps)
+    torch.cuda.synchronize()
+    eta_res = float(((ql[0] + bl) - 100.0).abs().max())
+    vel_res = float((ql[1:3].abs() / ql[0]).max())
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+    total = world * dofs * 5 * steps
+    v32 = total / (ms32 * 1e-3)
+    v64 = total / (ms64 * 1e-3)
+    vseq = dofs_inst * nseq * 5 * steps / (ms_seq * 1e-3)
+    line = {
+        "metric": "DOF-stage updates/s", "value": v32, "unit": "DOF-stage/s", "n_gpus": world, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": ms32 / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64-state/f32-flux", "data": "synthetic",
+        "config": {"workload": f"{n_inst} rotating shallow-water instances, periodic 32x32 elements, N=4, EC "
+                               "volume + Rusanov surface flux, FP32 flux / FP64 state, LSRK54, one packed operator",
+                   "instances": n_inst, "dofs": dofs, "stages_per_step": 5,
+                   "l2": f"working set ~{3 * dofs * 8 / 1e9:.2f} GB > 126 MB L2 (no flush)",
+                   "elements_per_cta": {"fp32flux": E32, "fp64": E64}},
+        "packed_fp64": {"value": v64, "ms_per_step": ms64 / steps},
+        "plain_fp64_one_instance_at_a_time": {"value": vseq, "ms_per_step_per_instance": ms_seq / steps / nseq,
+                                               "sample_instances": nseq},
+        "speedup_vs_plain_fp64": v32 / vseq,
+        "accuracy_vs_fp64": {"rel_l2_max": float(err.max()), "rel_l2_median": float(err.median()),
+                             "mass_drift_max_fp32flux": float(drift32.max()),
+                             "mass_drift_max_fp64": float(drift64.max())},
+        "lake_at_rest_fp32flux": {"instances": nl, "max_abs_surface_residual_m": eta_res,
+                                  "max_abs_velocity_m_per_s": vel_res},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
 def profiled_traffic():
     """DRAM bytes (read + write) of one FP64 tendency launch of this workload,
     from the committed ncu summary of the same kernel and workload."""
@@ -365,14 +590,31 @@ def profiled_traffic():
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: 100 for the bubble, 500 for the shallow-water batch)")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32flux"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="bubble", choices=["bubble", "swbatch", "serve"],
+                    help="bubble: 3-D rising bubble, IMEX ARK23 (default); swbatch: packed shallow-water "
+                         "instances; serve: Poisson request stream through the serving loop")
+    ap.add_argument("--instances", type=int, default=256)
+    ap.add_argument("--requests", type=int, default=2000)
+    ap.add_argument("--rate", type=float, default=200.0)
+    ap.add_argument("--time-scale", type=float, default=0.002)
+    ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
+    ap.add_argument("--pool-elements", type=int, default=1 << 16)
+    ap.add_argument("--error-samples", type=int, default=16)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.workload == "swbatch":
+        return run_swbatch(args)
+    if args.workload == "serve":
+        return run_serve(args)
+    if args.steps is None:
+        args.steps = 100
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
