@@ -58,6 +58,7 @@ SIGNATURES = {
     "atb_op_create_pool": [C.POINTER(OpDesc), C.c_int, C.POINTER(C.c_void_p)],
     "atb_op_place_instance": [_VP, C.c_int, C.POINTER(OpDesc), _DP, _VP],
     "atb_op_set_active_elements": [_VP, C.c_int],
+    "atb_op_move_instance": [_VP, C.c_int, C.c_int, C.c_int, _VP, _VP],
     "atb_op_set_instance_aux": [_VP, C.c_int, _DP, _VP],
     "atb_op_copy_instance_aux": [_VP, C.c_int, C.c_int, _VP],
     "atb_op_apply": [_VP, PtrArr, PtrArr, C.c_double, C.c_int, _VP],

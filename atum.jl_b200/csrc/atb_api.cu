@@ -144,6 +144,9 @@ struct atb_op {
   std::vector<int> col_e0;    // bottom element of every vertical column
   bool cols_uniform = true;   // every instance has the same element counts
   int npre = 0, npv = 0;
+  void* h_geo = nullptr;        // page-locked geometry staging (pools)
+  size_t geo_bytes = 0;
+  cudaEvent_t geo_ev = nullptr;  // last copy out of h_geo
   std::vector<double> w, D;
   double* d_ginv = nullptr;
   int* d_nbr = nullptr;
@@ -272,6 +275,11 @@ extern "C" int atb_op_destroy(atb_op* op) {
   cudaFree(op->d_partials);
   cudaFree(op->d_red);
   if (op->h_red) cudaFreeHost(op->h_red);
+  if (op->geo_ev) {
+    cudaEventSynchronize(op->geo_ev);
+    cudaEventDestroy(op->geo_ev);
+  }
+  if (op->h_geo) cudaFreeHost(op->h_geo);
   delete op;
   return ATB_OK;
 }
@@ -305,9 +313,10 @@ bool same_kind(const atb_op_desc* a, const atb_op_desc* b) {
 
 // Geometry of one instance whose elements start at `off` in the packed
 // ordering: 2/h per dimension, Jacobian determinant, neighbour table
-// (absolute element, or -(face number) on a non-periodic boundary), and the
-// bottom element of every vertical column.  Outputs hold the instance's own
-// elements only (element off + e at index e).
+// (neighbour element minus own element, or NBR_BOUNDARY + face number on a
+// non-periodic boundary: the same wherever the instance sits), and the bottom
+// element of every vertical column.  Outputs hold the instance's own elements
+// only (element off + e at index e).
 int instance_geometry(const atb_op_desc* di, int off, double* ginv, double* J, int* nbr, std::vector<int>* col_e0) {
   const int dim = di->dim;
   int Kd[3] = {1, 1, 1};
@@ -339,18 +348,18 @@ int instance_geometry(const atb_op_desc* di, int off, double* ginv, double* J, i
         for (int k = 0; k < 3; ++k)
           for (int f = 0; f < 2; ++f) {
             const int face = 2 * k + f;
-            if (k >= dim) { nbr[e * 6 + face] = -(face + 1); continue; }
+            if (k >= dim) { nbr[e * 6 + face] = NBR_BOUNDARY + face + 1; continue; }
             int nb[3] = {idx[0], idx[1], idx[2]};
             nb[k] += f ? 1 : -1;
             if (nb[k] < 0 || nb[k] >= Kd[k]) {
               if (di->periodic[k]) {
                 nb[k] = (nb[k] + Kd[k]) % Kd[k];
               } else {
-                nbr[e * 6 + face] = -(face + 1);  // boundary tag = face number
+                nbr[e * 6 + face] = NBR_BOUNDARY + face + 1;  // boundary tag = face number
                 continue;
               }
             }
-            nbr[e * 6 + face] = off + elem_index(di, nb);
+            nbr[e * 6 + face] = elem_index(di, nb) - e;  // relative: position independent
           }
       }
   return ATB_OK;
@@ -578,6 +587,11 @@ extern "C" int atb_op_create_pool(const atb_op_desc* kind, int capacity_elements
   if (rc) return rc;
   (*out)->K_active = 0;
   (*out)->col_e0.clear();
+  if (cudaEventCreateWithFlags(&(*out)->geo_ev, cudaEventDisableTiming) != cudaSuccess) {
+    atb_op_destroy(*out);
+    *out = nullptr;
+    return fail(ATB_ERR_CUDA, "event creation failed");
+  }
   (*out)->cols_uniform = false;  // placements have their own grids: no banded solve
   return ATB_OK;
 }
@@ -597,22 +611,78 @@ extern "C" int atb_op_place_instance(atb_op* op, int first_element, const atb_op
     return fail(ATB_ERR_INVALID, "placement [%d, %ld) outside the pool's %d elements", first_element,
                 (long)first_element + Ki, op->K);
   if (op->naux > 0 && !aux_host) return fail(ATB_ERR_INVALID, "aux fields missing");
-  std::vector<double> ginv((size_t)Ki * 3), J(Ki);
-  std::vector<int> nbr((size_t)Ki * 6);
-  if (instance_geometry(desc, first_element, ginv.data(), J.data(), nbr.data(), nullptr))
-    return fail(ATB_ERR_INVALID, "vertex vectors of the placed instance are not increasing");
+  if (!op->geo_ev) return fail(ATB_ERR_INVALID, "instances are placed into pools (atb_op_create_pool)");
   cudaStream_t st = (cudaStream_t)stream;
-  // pageable-source async copies: the sources may be released on return
-  CK(cudaMemcpyAsync(op->d_ginv + (size_t)first_element * 3, ginv.data(), ginv.size() * sizeof(double),
+  // geometry through the pool's page-locked staging area (reused once the
+  // previous placement's copies have run): no pageable copy that could block
+  // the caller behind queued work
+  const size_t gbytes = (size_t)Ki * (4 * sizeof(double) + 6 * sizeof(int));
+  if (op->geo_bytes < gbytes) {
+    if (op->h_geo) {
+      CK(cudaEventSynchronize(op->geo_ev));
+      cudaFreeHost(op->h_geo);
+      op->h_geo = nullptr;
+    }
+    if (cudaHostAlloc(&op->h_geo, gbytes, cudaHostAllocDefault) != cudaSuccess) {
+      op->h_geo = nullptr;
+      op->geo_bytes = 0;
+      return fail(ATB_ERR_NOMEM, "page-locked geometry staging of %zu bytes failed", gbytes);
+    }
+    op->geo_bytes = gbytes;
+  } else {
+    CK(cudaEventSynchronize(op->geo_ev));
+  }
+  double* ginv = (double*)op->h_geo;
+  double* J = ginv + (size_t)Ki * 3;
+  int* nbr = (int*)(J + Ki);
+  if (instance_geometry(desc, first_element, ginv, J, nbr, nullptr))
+    return fail(ATB_ERR_INVALID, "vertex vectors of the placed instance are not increasing");
+  CK(cudaMemcpyAsync(op->d_ginv + (size_t)first_element * 3, ginv, (size_t)Ki * 3 * sizeof(double),
                      cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(op->d_J + first_element, J.data(), J.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(op->d_nbr + (size_t)first_element * 6, nbr.data(), nbr.size() * sizeof(int),
+  CK(cudaMemcpyAsync(op->d_J + first_element, J, (size_t)Ki * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(op->d_nbr + (size_t)first_element * 6, nbr, (size_t)Ki * 6 * sizeof(int),
                      cudaMemcpyHostToDevice, st));
+  CK(cudaEventRecord(op->geo_ev, st));
+  // aux: a pageable source is staged before the call returns; a page-locked
+  // one is read by the copy engine later and must outlive the copies
   const size_t n = (size_t)Ki * op->Np;
   for (int k = 0; k < op->naux; ++k)
     CK(cudaMemcpyAsync(op->d_aux + (size_t)k * op->stride() + (size_t)first_element * op->Np, aux_host + k * n,
                        n * sizeof(double), cudaMemcpyHostToDevice, st));
   return ATB_OK;
+}
+
+extern "C" int atb_op_move_instance(atb_op* op, int dst_first, int src_first, int n_elements, void* scratch,
+                                    void* stream) {
+  if (!op) return fail(ATB_ERR_INVALID, "null argument");
+  const int Ki = n_elements;
+  if (Ki < 0 || dst_first < 0 || src_first < 0 || (long)dst_first + Ki > op->K || (long)src_first + Ki > op->K)
+    return fail(ATB_ERR_INVALID, "move outside the pool's %d elements", op->K);
+  if (dst_first == src_first || Ki == 0) return ATB_OK;
+  const bool overlap = std::abs(dst_first - src_first) < Ki;
+  if (overlap && !scratch) return fail(ATB_ERR_INVALID, "overlapping move needs scratch");
+  cudaStream_t st = (cudaStream_t)stream;
+  // every per-element table is position independent (relative neighbours):
+  // a move is a device copy of rows, through scratch when the ranges overlap
+  auto move = [&](void* dst, const void* src, size_t bytes) -> int {
+    if (overlap) {
+      CK(cudaMemcpyAsync(scratch, src, bytes, cudaMemcpyDeviceToDevice, st));
+      CK(cudaMemcpyAsync(dst, scratch, bytes, cudaMemcpyDeviceToDevice, st));
+    } else {
+      CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, st));
+    }
+    return ATB_OK;
+  };
+  int rc;
+  const size_t n = (size_t)Ki * op->Np;
+  for (int k = 0; k < op->naux; ++k)
+    if ((rc = move(op->d_aux + (size_t)k * op->stride() + (size_t)dst_first * op->Np,
+                   op->d_aux + (size_t)k * op->stride() + (size_t)src_first * op->Np, n * sizeof(double))))
+      return rc;
+  if ((rc = move(op->d_ginv + (size_t)dst_first * 3, op->d_ginv + (size_t)src_first * 3, (size_t)Ki * 3 * sizeof(double))))
+    return rc;
+  if ((rc = move(op->d_J + dst_first, op->d_J + src_first, (size_t)Ki * sizeof(double)))) return rc;
+  return move(op->d_nbr + (size_t)dst_first * 6, op->d_nbr + (size_t)src_first * 6, (size_t)Ki * 6 * sizeof(int));
 }
 
 extern "C" int atb_op_set_active_elements(atb_op* op, int n_elements) {

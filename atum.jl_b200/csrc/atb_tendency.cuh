@@ -43,10 +43,15 @@ namespace atb {
 enum { VK_WEAK = 0, VK_CENTRAL = 1, VK_EC = 2, VK_KG = 3, VK_EC32 = 4 };
 enum { EPI_SET = 0, EPI_ADD = 1, EPI_LSRK = 2, EPI_SUBOUT2 = 3, EPI_RLSRK = 4 };
 
+// neighbour-table encoding: relative offsets for interior faces, so an
+// instance's rows move between element ranges unchanged; NBR_BOUNDARY + tag
+// (tag = face number 1..6) on a non-periodic boundary face
+constexpr int NBR_BOUNDARY = -2147483647 - 1;
+
 struct TendArgs {
   int K, Nq, Np, Nfp, E, naux;
   const double* ginv;  // K*3: 2/h_d per element
-  const int* nbr;      // K*6: neighbour element, or -(boundary tag)
+  const int* nbr;      // K*6: neighbour element - e, or NBR_BOUNDARY + tag
   const double* aux;   // naux * stride
   const double* tab;   // Cfd[Nq*Nq], Cw[Nq*Nq], lift_end
   LawP law;
@@ -268,9 +273,12 @@ __device__ __forceinline__ void face_task(const TendArgs& A, const LawP& L, int 
   for (int s = 0; s < NS; ++s) qm[s] = sq[s * Np + nm];
 #pragma unroll
   for (int k = 0; k < NAM; ++k) am[k] = (k < naux) ? sa[k * Np + nm] : 0.0;
-  const int nb = __ldg(A.nbr + 6 * e + face);
+  // neighbour table entries are relative (neighbour element - e), or a
+  // boundary tag offset by NBR_BOUNDARY
+  const int nv = __ldg(A.nbr + 6 * e + face);
   const double sgn = side ? 1.0 : -1.0;
-  if (nb >= 0) {
+  if (nv > NBR_BOUNDARY + 64) {
+    const int nb = e + nv;
     const int stride_d = (D_ == 0) ? 1 : (D_ == 1) ? Nq : Nq * Nq;
     const int pn = nm + (side ? -(Nq - 1) : (Nq - 1)) * stride_d;
     const size_t pid = (size_t)nb * Np + pn;
@@ -279,7 +287,7 @@ __device__ __forceinline__ void face_task(const TendArgs& A, const LawP& L, int 
 #pragma unroll
     for (int k = 0; k < NAM; ++k) ap[k] = (k < naux) ? __ldg(A.aux + k * A.stride + pid) : 0.0;
   } else {
-    boundary_state<LAW, DIM>(L, D_, sgn, -nb, qm, qp);
+    boundary_state<LAW, DIM>(L, D_, sgn, nv - NBR_BOUNDARY, qm, qp);
 #pragma unroll
     for (int k = 0; k < NAM; ++k) ap[k] = am[k];
   }

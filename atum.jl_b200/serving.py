@@ -48,7 +48,18 @@ import numpy as np
 from . import _lib
 from ._device import make_desc
 
-__all__ = ["Request", "Server", "Stats", "kind_key", "pool_bytes_per_element"]
+__all__ = ["Request", "Server", "Stats", "kind_key", "pool_bytes_per_element", "pinned_array"]
+
+
+def pinned_array(a: np.ndarray) -> np.ndarray:
+    """A float64 copy of ``a`` in page-locked host memory (numpy view of a
+    pinned torch tensor): inputs held this way are admitted by DMA."""
+    import torch
+
+    t = torch.empty(a.shape, dtype=torch.float64).pin_memory()
+    out = t.numpy()
+    out[...] = a
+    return out
 
 _KIND_STAGES = {"LSRK54": 5, "LSRK144": 14}
 _GRID_FIELDS = ("K", "vertices", "periodic", "stacked")
@@ -62,6 +73,7 @@ class Request:
     dt: float
     nsteps: int
     arrival: float = 0.0       # seconds after the stream starts
+    keep_result: bool = True   # False: the final state is copied out, then dropped
     # filled by the server
     admitted: float = math.nan
     finished: float = math.nan
@@ -123,8 +135,37 @@ class _PoolDevice:
             self.h = None
 
 
+class _Staging:
+    """Pinned host buffers for input copies, reused once their copy has run."""
+
+    def __init__(self, limit_bytes: float = 8e9):
+        self.bufs = []   # [tensor, event or None]
+        self.limit = limit_bytes
+
+    def get(self, n: int):
+        import torch
+
+        for b in self.bufs:
+            if b[0].numel() >= n and (b[1] is None or b[1].query()):
+                return b
+        held = sum(b[0].numel() * 8 for b in self.bufs)
+        if held + n * 8 > self.limit and self.bufs:
+            # wait for the oldest copy, then replace its buffer if too small
+            b = self.bufs.pop(0)
+            if b[1] is not None:
+                b[1].synchronize()
+            if b[0].numel() < n:
+                b = [torch.empty(n, dtype=torch.float64, pin_memory=True), None]
+            self.bufs.append(b)
+            return b
+        b = [torch.empty(max(n, 1 << 20), dtype=torch.float64, pin_memory=True), None]
+        self.bufs.append(b)
+        return b
+
+
 class _Pool:
-    def __init__(self, key, template, capacity: int, chunk: int, kind: str, max_tick_steps: int):
+    def __init__(self, key, template, capacity: int, chunk: int, kind: str, max_tick_steps: int,
+                 copy_stream=None, staging=None):
         import torch
 
         from .odesolvers import Solver
@@ -143,13 +184,21 @@ class _Pool:
         self._dev = _PoolDevice(h, self.ns)
         self.cuda = torch.device("cuda", torch.cuda.current_device())
         self.stream = torch.cuda.Stream(device=self.cuda)
+        # inputs arrive on a copy stream, so admission never waits for the
+        # pool's launches; the pool stream waits for those copies
+        self.copy_stream = copy_stream if copy_stream is not None else torch.cuda.Stream(device=self.cuda)
+        self.staging = staging if staging is not None else _Staging()
+        self.pending = []
         self.q = torch.zeros((self.ns, self.capacity, self.Np), dtype=torch.float64, device=self.cuda)
         self.solver = Solver(kind, self, 1.0)
         # one time step per element (0 past the last request), a fixed device
         # pointer read by every stage, so captured graphs see updates
         self.dte = torch.zeros(self.capacity, dtype=torch.float64, device=self.cuda)
-        self.dte_pinned = torch.zeros(self.capacity, dtype=torch.float64).pin_memory()
-        self._dt_event = None
+        # pinned host copies used in turn, so a refresh rarely waits for an
+        # earlier transfer
+        self.dte_pinned = [torch.zeros(self.capacity, dtype=torch.float64, pin_memory=True) for _ in range(4)]
+        self._dt_events = [None] * 4
+        self._dt_turn = 0
         _lib.check(_lib.lib().atb_solver_set_element_dt(
             self.solver.h, C.cast(C.c_void_p(self.dte.data_ptr()), _lib._DP)))
         self.placed: List[_Placed] = []
@@ -159,7 +208,10 @@ class _Pool:
         self.dof_stage_updates = 0
         self.warm = set()
         self.dirty = True
-        self.staging = []
+        self.inflight = []       # (event, [(request, pinned view)], buffer) per tick
+        self.inflight_prefix = 0
+        self.naux = template.descriptor_fields()["naux"]
+        self.host = {"dt": 0.0, "launch": 0.0, "results": 0.0, "compact": 0.0}
 
     # a Solver binds to a pool as to an operator
     @property
@@ -176,32 +228,53 @@ class _Pool:
         self.q = self.dte = None
         torch.cuda.empty_cache()
 
+    def _free_start(self) -> int:
+        # past the used prefix and past every launch still in flight
+        return max(self._launched(), self.inflight_prefix if self.inflight else 0)
+
     def room(self) -> int:
-        return self.capacity - self.used
+        return self.capacity - self._free_start()
 
     # admission ----------------------------------------------------------
-    def _place(self, p: _Placed):
+    def _place(self, p: _Placed, stream):
         _lib.check(_lib.lib().atb_op_place_instance(self._dev.h, p.first, C.byref(p.desc),
                                                     _lib.dptr(p.aux) if p.aux.size else None,
-                                                    _lib.stream_ptr(self.stream)))
+                                                    _lib.stream_ptr(stream)))
 
     def admit(self, r: Request, now: float):
         import torch
 
-        p = _Placed(r, self.used)
+        # the new range starts past every launch in flight (the launched
+        # prefix), so the copy stream writes nothing a running stage touches
+        p = _Placed(r, self._free_start())
         K = p.K
-        with torch.cuda.stream(self.stream):
-            self._place(p)
-            src = torch.from_numpy(np.ascontiguousarray(r.q0, dtype=np.float64).reshape(self.ns, K, self.Np))
-            stage = src.pin_memory()
-            self.q[:, p.first:p.first + K].copy_(stage, non_blocking=True)
-            # the pinned staging buffer lives until its copy has run
-            self.staging.append((stage, torch.cuda.current_stream().record_event()))
-        self.staging = [(s, e) for s, e in self.staging if not e.query()]
+        n = self.ns * K * self.Np
+        src = None
+        if isinstance(r.q0, np.ndarray) and r.q0.dtype == np.float64 and r.q0.flags.c_contiguous:
+            t = torch.from_numpy(r.q0.reshape(-1))
+            if t.is_pinned():
+                src = t       # page-locked input: one DMA, no staging copy
+        b = None
+        if src is None:
+            b = self.staging.get(n)
+            src = b[0][:n]
+            src.numpy()[:] = np.asarray(r.q0, dtype=np.float64).reshape(-1)
+        with torch.cuda.stream(self.copy_stream):
+            self._place(p, self.copy_stream)
+            self.q[:, p.first:p.first + K].copy_(src.view(self.ns, K, self.Np), non_blocking=True)
+            ev = self.copy_stream.record_event()
+        if b is not None:
+            b[1] = ev
+        self.pending.append(ev)
         self.placed.append(p)
-        self.used += K
+        self.used = p.first + K
         r.admitted = now
         self.dirty = True
+
+    def _join_copies(self):
+        for ev in self.pending:
+            self.stream.wait_event(ev)
+        self.pending = []
 
     # stepping -----------------------------------------------------------
     def _launched(self) -> int:
@@ -217,25 +290,32 @@ class _Pool:
     def _refresh_dt(self):
         import torch
 
-        # the previous transfer out of the pinned buffer must have run
-        if self._dt_event is not None:
-            self._dt_event.synchronize()
-        host = self.dte_pinned.numpy()
+        i = self._dt_turn
+        self._dt_turn = (i + 1) % len(self.dte_pinned)
+        if self._dt_events[i] is not None:
+            self._dt_events[i].synchronize()
+        host = self.dte_pinned[i].numpy()
         host[:] = 0.0
         for p in self.placed:
             host[p.first:p.first + p.K] = p.req.dt
-        self.dte.copy_(self.dte_pinned, non_blocking=True)
-        self._dt_event = torch.cuda.current_stream().record_event()
+        self.dte.copy_(self.dte_pinned[i], non_blocking=True)
+        self._dt_events[i] = torch.cuda.current_stream().record_event()
         self.dirty = False
 
     def tick(self, use_graphs: bool) -> int:
+        """Launch S steps of every placed request, then (same stream) the
+        copies of the requests that finish with them and the moves that
+        close their gaps.  Nothing waits here; ``poll`` collects results."""
         import torch
 
         S = self.tick_steps()
         n = self._launched()
+        self._join_copies()
+        t0 = time.perf_counter()
         with torch.cuda.stream(self.stream):
             if self.dirty:
                 self._refresh_dt()
+            t1 = time.perf_counter()
             _lib.check(_lib.lib().atb_op_set_active_elements(self._dev.h, n))
             key = (n, S)
             g = self.graphs.get(key) if use_graphs else None
@@ -246,35 +326,52 @@ class _Pool:
                 self.solver.step(self.q, S, stream=self.stream)
                 self.warm.add(key)
             else:
+                # capture_begin/end directly: the torch.cuda.graph context
+                # manager also synchronises, collects garbage and empties the
+                # allocator cache on every capture
                 g = torch.cuda.CUDAGraph()
-                with torch.cuda.graph(g, stream=self.stream, capture_error_mode="thread_local"):
+                g.capture_begin(capture_error_mode="thread_local")
+                try:
                     self.solver.step(self.q, S, stream=self.stream)
+                finally:
+                    g.capture_end()
                 self.graphs[key] = g
                 g.replay()
+        t2 = time.perf_counter()
+        useful = sum(p.K for p in self.placed)
+        self.dof_stage_updates += self.ns * useful * self.Np * _KIND_STAGES[self.kind] * S
         for p in self.placed:
             p.remaining -= S
-        self.dof_stage_updates += self.ns * self.used * self.Np * _KIND_STAGES[self.kind] * S
+        self.inflight_prefix = max(self.inflight_prefix, n)
+        fin = [p for p in self.placed if p.remaining <= 0]
+        outs = []
+        buf = None
+        if fin:
+            tot = sum(self.ns * p.K * self.Np for p in fin)
+            buf = torch.empty(tot, dtype=torch.float64, pin_memory=True)
+            o = 0
+            with torch.cuda.stream(self.stream):
+                for p in fin:
+                    m = self.ns * p.K * self.Np
+                    v = buf[o:o + m].view(self.ns, p.K, self.Np)
+                    v.copy_(self.q[:, p.first:p.first + p.K], non_blocking=True)
+                    outs.append((p.req, v))
+                    o += m
+            t3 = time.perf_counter()
+            self._compact()
+            self.host["results"] += t3 - t2
+            self.host["compact"] += time.perf_counter() - t3
+        ev = self.stream.record_event()
+        self.host["dt"] += t1 - t0
+        self.host["launch"] += t2 - t1
+        self.inflight.append((ev, outs, buf))
         return S
 
-    def retire(self, now_fn, done: List[Request]):
-        """Copy finished requests to the host; move the rest down."""
+    def _compact(self):
+        """Move the unfinished requests down over the finished ones (on the
+        pool stream, after the result copies)."""
         import torch
 
-        fin = [p for p in self.placed if p.remaining <= 0]
-        if not fin:
-            return
-        outs = []
-        with torch.cuda.stream(self.stream):
-            for p in fin:
-                h = torch.empty((self.ns, p.K, self.Np), dtype=torch.float64).pin_memory()
-                h.copy_(self.q[:, p.first:p.first + p.K], non_blocking=True)
-                outs.append((p, h))
-        self.stream.synchronize()
-        t = now_fn()
-        for p, h in outs:
-            p.req.result = h.numpy()
-            p.req.finished = t
-            done.append(p.req)
         keep = [p for p in self.placed if p.remaining > 0]
         first = 0
         with torch.cuda.stream(self.stream):
@@ -282,12 +379,43 @@ class _Pool:
                 if p.first != first:
                     src = self.q[:, p.first:p.first + p.K].clone()
                     self.q[:, first:first + p.K].copy_(src)
+                    scratch = None
+                    if p.first - first < p.K:
+                        nb = p.K * (8 * self.Np * self.naux + 56)
+                        scratch = torch.empty(nb, dtype=torch.uint8, device=self.cuda)
+                    _lib.check(_lib.lib().atb_op_move_instance(
+                        self._dev.h, first, p.first, p.K,
+                        C.c_void_p(scratch.data_ptr()) if scratch is not None else None,
+                        _lib.stream_ptr(self.stream)))
                     p.first = first
-                    self._place(p)
                 first += p.K
         self.placed = keep
         self.used = first
         self.dirty = True
+
+    def busy(self) -> bool:
+        return bool(self.inflight)
+
+    def poll(self, now_fn, done: List[Request], wait: bool = False) -> int:
+        """Collect the ticks that have completed (the oldest one waited for
+        when ``wait``); returns how many completed."""
+        k = 0
+        while self.inflight:
+            ev, outs, buf = self.inflight[0]
+            if not ev.query():
+                if not (wait and k == 0):
+                    break
+                ev.synchronize()
+            self.inflight.pop(0)
+            t = now_fn()
+            for r, v in outs:
+                r.result = v.numpy().copy() if r.keep_result else None
+                r.finished = t
+                done.append(r)
+            k += 1
+        if not self.inflight:
+            self.inflight_prefix = 0
+        return k
 
 
 @dataclass
@@ -307,12 +435,26 @@ class Stats:
 class Server:
     """Continuous-batching server for LSRK time stepping of many problems."""
 
-    def __init__(self, hbm_budget_bytes: float = 150e9, capacity: int = 1 << 16, chunk: int = 256,
-                 kind: str = "LSRK54", max_tick_steps: int = 16, use_graphs: bool = True):
+    def __init__(self, hbm_budget_bytes: float = 150e9, capacity: Optional[int] = None, chunk: int = 256,
+                 kind: str = "LSRK54", max_tick_steps: int = 16, use_graphs: bool = True,
+                 pool_bytes: Optional[float] = None, max_pool_elements: int = 1 << 18):
+        """``capacity``: elements per pool (fixed); otherwise a pool holds
+        ``pool_bytes`` (default: an eighth of the budget) worth of elements of
+        its kind, at most ``max_pool_elements`` and at least the request that
+        opens it.  Inputs held in page-locked host memory (``pinned_array``)
+        are copied by DMA straight from the caller's buffer, which must stay
+        unchanged while the server runs; others go through pinned staging."""
         if kind not in _KIND_STAGES:
             raise ValueError("the server steps with LSRK54 or LSRK144")
         self.budget = float(hbm_budget_bytes)
-        self.capacity = int(capacity)
+        self.capacity = None if capacity is None else int(capacity)
+        self.pool_budget = float(pool_bytes) if pool_bytes is not None else self.budget / 8
+        self.max_pool_elements = int(max_pool_elements)
+        self._keys = {}
+        self.max_inflight = 2
+        self._copy_stream = None
+        self._staging = _Staging()
+        self.timers = {"admit": 0.0, "new_pool": 0.0, "tick": 0.0, "poll": 0.0, "release": 0.0}
         self.chunk = int(chunk)
         self.kind = kind
         self.max_tick_steps = int(max_tick_steps)
@@ -327,7 +469,7 @@ class Server:
         for k in list(self.pools):
             keep = []
             for p in self.pools[k]:
-                if not p.placed and self.pool_bytes + need > self.budget:
+                if not p.placed and not p.inflight and self.pool_bytes + need > self.budget:
                     self.pool_bytes -= p.nbytes
                     self.retired_updates += p.dof_stage_updates
                     p.close()
@@ -338,20 +480,37 @@ class Server:
             else:
                 del self.pools[k]
 
+    def _pool_capacity(self, dg) -> int:
+        if self.capacity is not None:
+            return self.capacity
+        fit = int(self.pool_budget // pool_bytes_per_element(dg))
+        return max(dg.grid.K, min(self.max_pool_elements, fit))
+
     def _find_pool(self, r: Request) -> Optional[_Pool]:
-        key = kind_key(r.dg)
+        key = self._keys.get(id(r.dg))
+        if key is None:
+            key = self._keys[id(r.dg)] = kind_key(r.dg)
         K = r.dg.grid.K
-        if K > self.capacity:
+        if self.capacity is not None and K > self.capacity:
             raise ValueError(f"request {r.rid} has {K} elements, more than a pool's {self.capacity}")
         for p in self.pools.get(key, []):
             if p.room() >= K:
                 return p
-        need = self.capacity * pool_bytes_per_element(r.dg)
+        cap = self._pool_capacity(r.dg)
+        need = cap * pool_bytes_per_element(r.dg)
         if self.pool_bytes + need > self.budget:
+            t = time.perf_counter()
             self._release_idle(need)
+            self.timers["release"] += time.perf_counter() - t
         if self.pool_bytes + need > self.budget:
             return None
-        p = _Pool(key, r.dg, self.capacity, self.chunk, self.kind, self.max_tick_steps)
+        t = time.perf_counter()
+        import torch
+
+        if self._copy_stream is None:
+            self._copy_stream = torch.cuda.Stream()
+        p = _Pool(key, r.dg, cap, self.chunk, self.kind, self.max_tick_steps, self._copy_stream, self._staging)
+        self.timers["new_pool"] += time.perf_counter() - t
         self.pools_made += 1
         self.pools.setdefault(key, []).append(p)
         self.pool_bytes += p.nbytes
@@ -374,31 +533,43 @@ class Server:
         now = lambda: time.perf_counter() - t0  # noqa: E731
         nxt = 0
         ticks = 0
+        pools = lambda: [p for ps in self.pools.values() for p in ps]  # noqa: E731
         while len(done) < len(reqs):
             tnow = now()
             while nxt < len(reqs) and reqs[nxt].arrival <= tnow:
                 queue.append(reqs[nxt])
                 nxt += 1
             waiting = []
+            ta = time.perf_counter()
             for r in queue:  # FIFO admission
                 p = self._find_pool(r)
                 if p is None:
                     waiting.append(r)
                 else:
                     p.admit(r, now())
+            self.timers["admit"] += time.perf_counter() - ta
             queue = waiting
-            busy = [p for ps in self.pools.values() for p in ps if p.placed]
-            if not busy:
-                if queue:
+            progressed = False
+            tt = time.perf_counter()
+            for p in pools():
+                if p.placed and len(p.inflight) < self.max_inflight:
+                    p.tick(self.use_graphs)
+                    ticks += 1
+                    progressed = True
+            tr = time.perf_counter()
+            self.timers["tick"] += tr - tt
+            for p in pools():
+                if p.inflight and p.poll(now, done):
+                    progressed = True
+            if not progressed:
+                busy = [p for p in pools() if p.inflight]
+                if busy:
+                    busy[0].poll(now, done, wait=True)
+                elif queue:
                     raise RuntimeError("a queued request fits no pool within the HBM budget")
-                if nxt < len(reqs):
+                elif nxt < len(reqs):
                     time.sleep(max(0.0, min(reqs[nxt].arrival - now(), 0.001)))
-                continue
-            for p in busy:
-                p.tick(self.use_graphs)
-            ticks += 1
-            for p in busy:
-                p.retire(now, done)
+            self.timers["poll"] += time.perf_counter() - tr
         torch.cuda.synchronize()
         span = now()
         lat = np.array([r.latency for r in done])
@@ -414,11 +585,19 @@ class Server:
         st.pools = self.pools_made
         st.ticks = ticks
         st.extra["dof_stage_updates"] = int(total)
+        st.extra["host_seconds"] = dict(self.timers)
+        for ps in self.pools.values():
+            for p in ps:
+                for k, v in p.host.items():
+                    st.extra["host_seconds"]["tick_" + k] = st.extra["host_seconds"].get("tick_" + k, 0.0) + v
         return st
 
     def close(self):
+        import torch
+
         for ps in self.pools.values():
             for p in ps:
                 p.close()
         self.pools.clear()
         self.pool_bytes = 0
+        torch.cuda.synchronize()

@@ -381,6 +381,9 @@ def run_serve(args):
             else:
                 c = P.bubble_3d(N=N, K=K, imex=False, precision=precision)
                 flow = 10e3 / 340.0                   # box / sound speed
+            # inputs in page-locked memory, as a client staging them for DMA
+            c.q0 = A.serving.pinned_array(c.q0)
+            c.dg._aux = A.serving.pinned_array(c.dg.auxstate_host())
             cache[key] = (c, flow)
         return cache[key]
 
@@ -394,18 +397,22 @@ def run_serve(args):
         c, flow = spec(kind, K, N, "fp32flux")
         tend = rng.uniform(0.5, 5.0) * flow * args.time_scale
         nsteps = max(1, int(math.ceil(tend / c.dt)))
-        reqs.append(A.serving.Request(rid=i, dg=c.dg, q0=c.q0, dt=c.dt, nsteps=nsteps, arrival=t))
-    srv = A.serving.Server(hbm_budget_bytes=args.hbm_budget_gb * 1e9, capacity=args.pool_elements,
-                           chunk=256, use_graphs=True)
+        reqs.append(A.serving.Request(rid=i, dg=c.dg, q0=c.q0, dt=c.dt, nsteps=nsteps, arrival=t,
+                                      keep_result=False))
+    sampled = reqs[:: max(1, len(reqs) // args.error_samples)][: args.error_samples]
+    for r in sampled:
+        r.keep_result = True
+    srv = A.serving.Server(hbm_budget_bytes=args.hbm_budget_gb * 1e9, chunk=256, use_graphs=True,
+                           pool_bytes=args.pool_gb * 1e9)
     # warm-up stream (a few requests), then the measured one
-    warm = [A.serving.Request(rid=-1 - j, dg=r.dg, q0=r.q0, dt=r.dt, nsteps=min(r.nsteps, 4), arrival=0.0)
-            for j, r in enumerate(reqs[:args.warmup])]
+    warm = [A.serving.Request(rid=-1 - j, dg=r.dg, q0=r.q0, dt=r.dt, nsteps=min(r.nsteps, 4), arrival=0.0,
+                              keep_result=False) for j, r in enumerate(reqs[:args.warmup])]
     srv.run(warm, realtime=False)
     with ClockSampler(torch.cuda.current_device()) as clk:
         st = srv.run(reqs, realtime=True)
     # accuracy: a sample of requests stepped alone in FP64
     errs = []
-    for r in reqs[:: max(1, len(reqs) // args.error_samples)][: args.error_samples]:
+    for r in sampled:
         kind = "vortex" if r.dg.law.dim == 2 else "bubble"
         c64, _ = spec(kind, int(round(r.dg.grid.Kd[0])), r.dg.grid.cell.N, "fp64")
         q = torch.as_tensor(c64.q0, device="cuda").contiguous()
@@ -429,10 +436,12 @@ def run_serve(args):
         "config": {"workload": "serving: Poisson stream of 2-D Euler vortices (16^2..128^2) and 3-D Euler-gravity "
                                "bubbles (8^3..32^3), N in 2..7, FP32 flux / FP64 state, LSRK54, packed by (law, N)",
                    "requests": args.requests, "rate_per_s": args.rate, "time_scale": args.time_scale,
-                   "hbm_budget_gb": args.hbm_budget_gb, "pool_elements": args.pool_elements},
+                   "hbm_budget_gb": args.hbm_budget_gb, "pool_gb": args.pool_gb},
         "latency_s": {"p50": st.p50_latency_s, "p99": st.p99_latency_s, "mean": st.mean_latency_s,
                       "max": float(lat.max())},
-        "makespan_s": st.makespan_s, "pools": st.pools, "ticks": st.ticks,
+        "makespan_s": st.makespan_s, "arrival_window_s": max(r.arrival for r in reqs),
+        "pools": st.pools, "ticks": st.ticks,
+        "host_seconds": st.extra["host_seconds"],
         "peak_pool_bytes": st.peak_pool_bytes, "dof_stage_updates": st.extra["dof_stage_updates"],
         "rel_l2_vs_fp64": {"samples": len(errs), "max": max(errs) if errs else None,
                            "median": float(np.median(errs)) if errs else None},
@@ -602,9 +611,9 @@ def main():
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--requests", type=int, default=2000)
     ap.add_argument("--rate", type=float, default=200.0)
-    ap.add_argument("--time-scale", type=float, default=0.002)
+    ap.add_argument("--time-scale", type=float, default=0.0005)
     ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
-    ap.add_argument("--pool-elements", type=int, default=1 << 16)
+    ap.add_argument("--pool-gb", type=float, default=12.0)
     ap.add_argument("--error-samples", type=int, default=16)
     args = ap.parse_args()
     if args.warmup < 3:

@@ -134,14 +134,23 @@ int atb_op_set_active(atb_op* op, int n_instances);
  * capacity_elements elements and none active.  atb_op_place_instance writes
  * the geometry (metrics, neighbour table offset by first_element) and aux
  * fields of the instance `desc` (same kind, any grid) into elements
- * [first_element, first_element + K) with copies ordered on `stream`; host
- * sources may be released on return.  atb_op_set_active_elements sets how
+ * [first_element, first_element + K) with copies ordered on `stream` (the
+ * geometry goes through the pool's own page-locked staging; a pageable aux
+ * source may be released on return, a page-locked one must stay valid until
+ * the copies have run).  atb_op_set_active_elements sets how
  * many leading elements tendency launches cover; a caller keeps its placed
  * instances inside that prefix.  Pools have no banded solve (ARK23). */
 int atb_op_create_pool(const atb_op_desc* kind, int capacity_elements, atb_op** out);
 int atb_op_place_instance(atb_op* op, int first_element, const atb_op_desc* desc, const double* aux_host,
                           void* stream);
 int atb_op_set_active_elements(atb_op* op, int n_elements);
+/* Moves n_elements elements (their metrics, neighbour rows and aux fields)
+ * from [src_first, +n) to [dst_first, +n) on the device, ordered on `stream`.
+ * Neighbour rows are stored relative to their element, so a placed instance
+ * moves unchanged.  Overlapping ranges go through `scratch`, device memory of
+ * n_elements * (8*Np*naux + 56) bytes (may be NULL otherwise).  The state
+ * fields are the caller's to move. */
+int atb_op_move_instance(atb_op* op, int dst_first, int src_first, int n_elements, void* scratch, void* stream);
 int atb_op_set_instance_aux(atb_op* op, int i, const double* aux_host, void* stream);
 int atb_op_copy_instance_aux(atb_op* op, int dst, int src, void* stream);
 /* Launch-shape tuning (no reference counterpart): times the tendency kernel

@@ -70,6 +70,8 @@ def test_budget_makes_pools_take_turns():
 
 def test_poisson_arrivals_realtime():
     reqs = _requests(10, rate=200.0)
+    for r in reqs[::2]:
+        r.q0 = A.serving.pinned_array(r.q0)     # DMA admission path
     srv = A.serving.Server(capacity=128, chunk=32)
     st = srv.run(reqs, realtime=True)
     assert st.requests == 10
