@@ -190,17 +190,37 @@ void fill_args(const atb_op* op, TendArgs& A) {
   A.a = 0;
   A.bdt = 0;
   A.dte = nullptr;
+  for (int j = 0; j < 3; ++j) {
+    for (int c = 0; c < 5; ++c) { A.acc[j][c] = nullptr; A.accin[j][c] = nullptr; }
+    A.ca[j] = A.cb[j] = 0.0;
+  }
+  A.adt = 0.0;
 }
+
+// EPI_ARK accumulators of one stage (see atb_tendency.cuh)
+struct ArkAcc {
+  double* acc[3][5];
+  const double* accin[3][5];
+  double ca[3], cb[3], adt;
+};
 
 // one tendency launch: epi with input q, outputs out/out2
 int run_tendency(atb_op* op, int epi, const double* const* q, double* const* out, double* const* out2, double a,
-                 double bdt, cudaStream_t st, const double* dte = nullptr) {
+                 double bdt, cudaStream_t st, const double* dte = nullptr, const ArkAcc* ark = nullptr) {
   TendArgs A;
   fill_args(op, A);
   A.epi = epi;
   A.a = a;
   A.bdt = bdt;
   A.dte = dte;
+  if (ark) {
+    for (int j = 0; j < 3; ++j) {
+      for (int c = 0; c < 5; ++c) { A.acc[j][c] = ark->acc[j][c]; A.accin[j][c] = ark->accin[j][c]; }
+      A.ca[j] = ark->ca[j];
+      A.cb[j] = ark->cb[j];
+    }
+    A.adt = ark->adt;
+  }
   for (int s = 0; s < 5; ++s) {
     A.q[s] = q[s < op->ns ? s : 0];
     A.out[s] = out ? out[s < op->ns ? s : 0] : nullptr;
@@ -512,11 +532,12 @@ int op_create_impl(const atb_op_desc* descs, int n, const double* const* aux_hos
   if (d->law == LAW_LEG) nu = dim + 3;
   if (d->law == LAW_SW && d->sw_topography) nu = (vk == VK_WEAK) ? dim + 1 : 1;
   op->naux_used = std::min(nu, op->naux);
-  // launch shape: E elements per CTA, ~256 threads (>= 1 element); the
+  // launch shape: E elements per CTA, ~128 threads (>= 1 element; the
+  // shape the autotuner picks on B200 for most orders); the
   // autotuner (atb_op_autotune) may pick another E
   op->npre = npre_of(d->law, dim, vk);
   op->npv = npv_stride_of(d->law, dim, vk);
-  op->E = std::max(1, 256 / Np);
+  op->E = std::max(1, 128 / Np);
   while (op->E > 1 && op_smem(op, op->E) > 100 * 1024) --op->E;
   op->smem = op_smem(op, op->E);
   if (op->smem > 227 * 1024) {
@@ -1110,7 +1131,85 @@ int rlsrk_step(atb_solver* s, double* const* q, cudaStream_t st) {
   return ATB_OK;
 }
 
+// ARK23 with split_rhs = false and the banded implicit solve, accumulated:
+// stage i's linear-operator launch (EPI_ARK) turns N(Q_i) and L(Q_i) into the
+// stage's explicit / implicit tendencies in registers and adds them straight
+// into the right-hand sides of the later stages and into the final update, so
+// no stage tendency is ever stored, the banded solve reads one ready
+// right-hand side, and no separate combination kernel runs.  The additions
+// happen in the same order as in ark_step, so the results are identical.
+int ark_step_accumulated(atb_solver* s, double* const* q, cudaStream_t st) {
+  const int ns = s->ns;
+  const size_t n = s->stride;
+  double *Q1[5], *Q2[5], *N[5], *R1[5], *R2[5], *F[5];
+  field_ptrs(s->Qs, ns, n, Q1);
+  field_ptrs(s->Qs + (size_t)ns * n, ns, n, Q2);
+  field_ptrs(s->exK, ns, n, N);
+  field_ptrs(s->imK, ns, n, R1);
+  field_ptrs(s->imK + (size_t)ns * n, ns, n, R2);
+  field_ptrs(s->imK + (size_t)2 * ns * n, ns, n, F);
+  double* qq[5];
+  for (int k = 0; k < 5; ++k) qq[k] = q[k < ns ? k : 0];
+  auto acc_clear = [](ArkAcc& a) {
+    for (int j = 0; j < 3; ++j) {
+      for (int c = 0; c < 5; ++c) { a.acc[j][c] = nullptr; a.accin[j][c] = nullptr; }
+      a.ca[j] = a.cb[j] = 0.0;
+    }
+  };
+  auto set = [&](ArkAcc& a, int j, double* const* dst, double* const* src, double ca, double cb) {
+    for (int c = 0; c < 5; ++c) {
+      a.acc[j][c] = dst[c];
+      a.accin[j][c] = src ? src[c] : nullptr;
+    }
+    a.ca[j] = ca;
+    a.cb[j] = cb;
+  };
+  auto solve = [&](double* const* R, double* const* Qout) -> int {
+    BandSolve B{};
+    B.M = s->M;
+    B.band = s->band;
+    B.blk = s->blk;
+    B.ld = s->ld;
+    B.npairs = 0;
+    B.dt = s->dt;
+    for (int c = 0; c < 5; ++c) { B.q[c] = R[c]; B.out[c] = Qout[c]; }
+    {
+      ProfScope ps(ATB_PROF_BAND, st);
+      launch_band_solve(B, st);
+    }
+    return check_launch("band solve");
+  };
+  int rc;
+  ArkAcc a;
+  // stage 1 (Q = q): R1, R2, F from q
+  if ((rc = run_tendency(s->rhs, EPI_SET, qq, N, nullptr, 0, 0, st))) return rc;
+  acc_clear(a);
+  a.adt = s->dt;
+  set(a, 0, R1, nullptr, s->exa[1][0], s->ima[1][0]);
+  set(a, 1, R2, nullptr, s->exa[2][0], s->ima[2][0]);
+  set(a, 2, F, nullptr, s->exb[0], s->imb[0]);
+  if ((rc = run_tendency(s->lin, EPI_ARK, qq, N, nullptr, 0, 0, st, nullptr, &a))) return rc;
+  // stage 2
+  if ((rc = solve(R1, Q1))) return rc;
+  if ((rc = run_tendency(s->rhs, EPI_SET, Q1, N, nullptr, 0, 0, st))) return rc;
+  acc_clear(a);
+  a.adt = s->dt;
+  set(a, 0, R2, R2, s->exa[2][1], s->ima[2][1]);
+  set(a, 1, F, F, s->exb[1], s->imb[1]);
+  if ((rc = run_tendency(s->lin, EPI_ARK, Q1, N, nullptr, 0, 0, st, nullptr, &a))) return rc;
+  // stage 3 and the update of q
+  if ((rc = solve(R2, Q2))) return rc;
+  if ((rc = run_tendency(s->rhs, EPI_SET, Q2, N, nullptr, 0, 0, st))) return rc;
+  acc_clear(a);
+  a.adt = s->dt;
+  set(a, 0, qq, F, s->exb[2], s->imb[2]);
+  if ((rc = run_tendency(s->lin, EPI_ARK, Q2, N, nullptr, 0, 0, st, nullptr, &a))) return rc;
+  s->time += s->dt;
+  return ATB_OK;
+}
+
 int ark_step(atb_solver* s, double* const* q, cudaStream_t st) {
+  if (s->rhs && s->lin && !s->split_rhs && s->band) return ark_step_accumulated(s, q, st);
   const int ns = s->ns;
   const size_t n = s->stride;
   double *Q[3][5], *ex[3][5], *im[3][5];

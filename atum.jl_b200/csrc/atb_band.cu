@@ -358,6 +358,391 @@ template <int NQ, int NS> void block_launch(const BandSolve& B, cudaStream_t st)
   band_solve_block_kernel<NQ, NS, LPB><<<(B.M.nlines + LPB - 1) / LPB, NQ * LPB, smem, st>>>(B, B.blk);
 }
 
+// Row-parallel form of the block recurrence: one thread per (row, line),
+// rows = the BW1 unknowns (node kv, state s) of one element of a vertical line,
+// lines fastest within a warp (LPB lines of a CTA -> consecutive horizontal
+// nodes -> coalesced field accesses).  Per element step a thread forms one row
+// of A_e v - C_e w (2*BW1 FMAs) from the staged blocks (two distinct rows per
+// warp -> broadcasts) and the line's vectors in shared memory; the CTA holds
+// BW1*LPB threads, so a step is short and many warps hide the latency of the
+// sequential element chain.  Field pointers are selected once per thread with
+// compile-time indices (a runtime-indexed kernel-parameter array would be
+// copied to local memory).
+template <int NQ, int NS, int LPB>
+__global__ void __launch_bounds__(NQ * NS * LPB) band_solve_rows_kernel(const BandSolve B, const double* blk) {
+  constexpr int BW1 = NQ * NS;
+  constexpr int MAT = BW1 * BW1;
+  constexpr int NT = BW1 * LPB;
+  extern __shared__ __align__(16) double sm[];
+  auto smat = [&](int b) { return sm + b * 2 * MAT; };
+  double* vb = sm + 4 * MAT;       // [BW1][LPB]: right-hand side (forward) / y (backward)
+  double* wb = vb + BW1 * LPB;     // [2][BW1][LPB]: previous element's result
+  const LineMap& M = B.M;
+  const int l = threadIdx.x % LPB, row = threadIdx.x / LPB;
+  const int kv = row / NS, s = row - kv * NS;
+  const int line = blockIdx.x * LPB + l;
+  const bool act = line < M.nlines;
+  const int KV = M.KV, nh = M.nh, Np = M.Np;
+  const int hn = act ? line % nh : 0;
+  const int e0 = act ? M.e0[line] : 0;
+  const double *pq = B.q[0], *pe0 = B.ex[0][0], *pi0 = B.im[0][0], *pe1 = B.ex[1][0], *pi1 = B.im[1][0];
+  double* po = B.out[0];
+#pragma unroll
+  for (int c = 1; c < NS; ++c)
+    if (c == s) {
+      pq = B.q[c];
+      pe0 = B.ex[0][c];
+      pi0 = B.im[0][c];
+      pe1 = B.ex[1][c];
+      pi1 = B.im[1][c];
+      po = B.out[c];
+    }
+  const int npairs = B.npairs;
+  const double dt = B.dt, a0 = B.a[0], b0 = B.b[0], a1 = B.a[1], b1 = B.b[1];
+  auto gidx = [&](int ev) { return (size_t)(e0 + ev * M.estep) * Np + hn + (size_t)nh * kv; };
+  auto stage = [&](double* dst, const double* src) {
+    for (int c = threadIdx.x; c < MAT; c += NT) cp_async16(dst + 2 * c, src + 2 * c);  // 2*MAT doubles
+  };
+  auto rhs = [&](int ev) {
+    if (!act) return 0.0;
+    const size_t g = gidx(ev);
+    double v = pq[g];
+    if (npairs > 0) v = v + dt * (a0 * pe0[g] + b0 * pi0[g]);
+    if (npairs > 1) v = v + dt * (a1 * pe1[g] + b1 * pi1[g]);
+    return v;
+  };
+  // y = A v - C w for this thread's row (same summation order as the
+  // register-window form: two sums, then their difference)
+  auto row_dot = [&](const double* Am, const double* Cm, const double* w) {
+    double acc = 0.0, acc2 = 0.0;
+#pragma unroll
+    for (int k = 0; k < BW1; ++k) {
+      acc += Am[row * BW1 + k] * vb[k * LPB + l];
+      acc2 += Cm[row * BW1 + k] * w[k * LPB + l];
+    }
+    return acc - acc2;
+  };
+  // ------------------------------------------------------------ forward
+  stage(smat(0), blk);
+  cp_async_commit();
+  if (KV > 1) stage(smat(1), blk + (size_t)4 * MAT);
+  cp_async_commit();
+  wb[row * LPB + l] = 0.0;  // y_{-1} = 0
+  wb[BW1 * LPB + row * LPB + l] = 0.0;
+  double bnext = rhs(0);
+  for (int ev = 0; ev < KV; ++ev) {
+    vb[row * LPB + l] = bnext;
+    if (ev + 1 < KV) bnext = rhs(ev + 1);
+    cp_async_wait1();
+    __syncthreads();
+    const double y = row_dot(smat(ev & 1), smat(ev & 1) + MAT, wb + ((ev + 1) & 1) * BW1 * LPB);
+    wb[(ev & 1) * BW1 * LPB + row * LPB + l] = y;
+    if (act) po[gidx(ev)] = y;
+    __syncthreads();
+    if (ev + 2 < KV) stage(smat(ev & 1), blk + (size_t)(ev + 2) * 4 * MAT);
+    cp_async_commit();
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  __syncthreads();
+  // ----------------------------------------------------------- backward
+  stage(smat(0), blk + (size_t)(KV - 1) * 4 * MAT + 2 * MAT);
+  cp_async_commit();
+  if (KV > 1) stage(smat(1), blk + (size_t)(KV - 2) * 4 * MAT + 2 * MAT);
+  cp_async_commit();
+  wb[row * LPB + l] = 0.0;  // x_{KV} = 0
+  wb[BW1 * LPB + row * LPB + l] = 0.0;
+  // this thread wrote y_e at exactly the address it reads back
+  double ynext = act ? po[gidx(KV - 1)] : 0.0;
+  for (int t = 0; t < KV; ++t) {
+    const int ev = KV - 1 - t;
+    vb[row * LPB + l] = ynext;
+    if (ev > 0) ynext = act ? po[gidx(ev - 1)] : 0.0;
+    cp_async_wait1();
+    __syncthreads();
+    const double x = row_dot(smat(t & 1), smat(t & 1) + MAT, wb + ((t + 1) & 1) * BW1 * LPB);
+    wb[(t & 1) * BW1 * LPB + row * LPB + l] = x;
+    if (act) po[gidx(ev)] = x;
+    __syncthreads();
+    if (t + 2 < KV) stage(smat(t & 1), blk + (size_t)(KV - 3 - t) * 4 * MAT + 2 * MAT);
+    cp_async_commit();
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+template <int NQ, int NS>
+void rows_launch(const BandSolve& B, cudaStream_t st) {
+  constexpr int BW1 = NQ * NS;
+  constexpr int LPB = 16;
+  constexpr size_t smem = sizeof(double) * (4 * BW1 * BW1 + 3 * BW1 * LPB);
+  static bool configured = false;
+  if (!configured && smem > 48 * 1024)
+    cudaFuncSetAttribute(band_solve_rows_kernel<NQ, NS, LPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  configured = true;
+  band_solve_rows_kernel<NQ, NS, LPB><<<(B.M.nlines + LPB - 1) / LPB, BW1 * LPB, smem, st>>>(B, B.blk);
+}
+
+template <int NS> solve_fn pick_rows(int nq) {
+  switch (nq) {
+    case 2: return rows_launch<2, NS>;
+    case 3: return rows_launch<3, NS>;
+    case 4: return rows_launch<4, NS>;
+    case 5: return rows_launch<5, NS>;
+    case 6: return rows_launch<6, NS>;
+    case 7: return rows_launch<7, NS>;
+    case 8: return rows_launch<8, NS>;
+  }
+  return nullptr;
+}
+
+// FP64 matrix-unit form of the block recurrence (mma.sync m8n8k4 f64; the
+// tcgen05 tensor cores have no FP64 kind).  A CTA owns LPC = 8*NT lines and
+// one warp per 8-row tile of the BW1 element rows; per element step a warp
+// computes its rows of Y = A_e V - C_e W for all LPC lines as KT x NT x 2
+// matrix-unit operations: A_e / C_e fragments come straight from the
+// (L1/L2-resident) block inverses into registers, prefetched one element ahead,
+// V (right-hand side) and W (previous element's result) are B fragments read
+// from shared memory (double-buffered, one barrier per element).  Rows are
+// padded to MT*8 and the reduction dimension to KT*4 with zeros.
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <int NQ, int NS, int NT, int D>
+__global__ void __launch_bounds__(32 * ((NQ * NS + 7) / 8)) band_solve_mma_kernel(const BandSolve B, const double* blk) {
+  constexpr int BW1 = NQ * NS;
+  constexpr int MAT = BW1 * BW1;
+  constexpr int MT = (BW1 + 7) / 8;  // warps
+  constexpr int KT = (BW1 + 3) / 4;
+  constexpr int KP = 4 * KT;
+  constexpr int LPC = 8 * NT;
+  constexpr int NTH = 32 * MT;
+  constexpr int NL = NQ * LPC;       // loader threads: one per (node kv, line)
+  // row stride of V / W: 4 doubles of padding put the 4 rows of a B fragment
+  // on distinct bank groups (2 wavefronts per fragment load, the minimum)
+  constexpr int LDV = LPC + 4;
+  extern __shared__ __align__(16) double sm[];
+  double* Vb = sm;                  // [2][KP][LDV]
+  double* Wb = sm + 2 * KP * LDV;   // [2][KP][LDV]
+  double* R = sm + 4 * KP * LDV;    // [D][5][NS][NL]: raw right-hand-side fields in flight
+  const LineMap& M = B.M;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, tq = lane & 3;
+  const int KV = M.KV, nh = M.nh, Np = M.Np;
+  const int line0 = blockIdx.x * LPC;
+  for (int i = threadIdx.x; i < 4 * KP * LDV; i += NTH) sm[i] = 0.0;
+  // ---- this thread's output rows: row = 8*warp + g, lines 8*nt + 2*tq + {0,1}
+  const int orow = 8 * warp + g;
+  const bool orow_ok = orow < BW1;
+  const int okv = orow_ok ? orow / NS : 0, os = orow_ok ? orow - okv * NS : 0;
+  double* po = B.out[0];
+#pragma unroll
+  for (int c = 1; c < NS; ++c)
+    if (c == os) po = B.out[c];
+  size_t obase[NT][2];
+  bool oact[NT][2];
+  const size_t ostep = (size_t)M.estep * Np;
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int line = line0 + 8 * nt + 2 * tq + i;
+      oact[nt][i] = orow_ok && line < M.nlines;
+      const int ln = oact[nt][i] ? line : 0;
+      obase[nt][i] = (size_t)M.e0[ln] * Np + ln % nh + (size_t)nh * okv;
+    }
+  // ---- loader: thread lt < NL owns node lkv of line ll for every state
+  const int lt = threadIdx.x;
+  const bool ld_ok = lt < NL;
+  const int lkv = ld_ok ? lt / LPC : 0, ll = ld_ok ? lt - lkv * LPC : 0;
+  const int lline = line0 + ll;
+  const bool lact = ld_ok && lline < M.nlines;
+  const size_t lbase = lact ? (size_t)M.e0[lline] * Np + lline % nh + (size_t)nh * lkv : 0;
+  const size_t lstep = (size_t)M.estep * Np;
+  const int npairs = B.npairs;
+  const double dt = B.dt, a0 = B.a[0], b0 = B.b[0], a1 = B.a[1], b1 = B.b[1];
+  auto rslot = [&](int slot, int f, int s) { return R + ((slot * 5 + f) * NS + s) * NL + lt; };
+  // raw fields of element ev into ring slot ev % D (the issuing thread is the
+  // only reader of what it copies: no barrier between copy and use)
+  auto issue_fwd = [&](int ev) {
+    if (lact && ev < KV) {
+      const size_t gi = lbase + (size_t)ev * lstep;
+      const int slot = ev % D;
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        cp_async8(rslot(slot, 0, s), B.q[s] + gi);
+        if (npairs > 0) {
+          cp_async8(rslot(slot, 1, s), B.ex[0][s] + gi);
+          cp_async8(rslot(slot, 2, s), B.im[0][s] + gi);
+        }
+        if (npairs > 1) {
+          cp_async8(rslot(slot, 3, s), B.ex[1][s] + gi);
+          cp_async8(rslot(slot, 4, s), B.im[1][s] + gi);
+        }
+      }
+    }
+    cp_async_commit();
+  };
+  auto combine_fwd = [&](int ev, int buf) {
+    if (!ld_ok) return;
+    const int slot = ev % D;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      double x = 0.0;
+      if (lact) {
+        x = *rslot(slot, 0, s);
+        if (npairs > 0) x = x + dt * (a0 * *rslot(slot, 1, s) + b0 * *rslot(slot, 2, s));
+        if (npairs > 1) x = x + dt * (a1 * *rslot(slot, 3, s) + b1 * *rslot(slot, 4, s));
+      }
+      Vb[(buf * KP + lkv * NS + s) * LDV + ll] = x;
+    }
+  };
+  auto issue_bwd = [&](int ev) {
+    if (lact && ev >= 0) {
+      const size_t gi = lbase + (size_t)ev * lstep;
+      const int slot = ev % D;
+#pragma unroll
+      for (int s = 0; s < NS; ++s) cp_async8(rslot(slot, 0, s), B.out[s] + gi);
+    }
+    cp_async_commit();
+  };
+  auto combine_bwd = [&](int ev, int buf) {
+    if (!ld_ok) return;
+    const int slot = ev % D;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) Vb[(buf * KP + lkv * NS + s) * LDV + ll] = lact ? *rslot(slot, 0, s) : 0.0;
+  };
+  // ---- A / C fragments: row 8*warp + g, column 4*kt + tq of a BW1 x BW1 block
+  auto frag = [&](const double* m, double* f) {
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt) {
+      const int c = 4 * kt + tq;
+      f[kt] = (orow_ok && c < BW1) ? __ldg(m + orow * BW1 + c) : 0.0;
+    }
+  };
+  auto step = [&](int buf, const double* fa, const double* fc, int ev) {
+    double acc[NT][2], acc2[NT][2];
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) acc[nt][0] = acc[nt][1] = acc2[nt][0] = acc2[nt][1] = 0.0;
+    const double* V = Vb + buf * KP * LDV;
+    const double* Wp = Wb + (buf ^ 1) * KP * LDV;
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt)
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt) {
+        const int k = 4 * kt + tq, n = 8 * nt + g;
+        dmma_8x8x4(acc[nt][0], acc[nt][1], fa[kt], V[k * LDV + n]);
+        dmma_8x8x4(acc2[nt][0], acc2[nt][1], fc[kt], Wp[k * LDV + n]);
+      }
+    double* W = Wb + buf * KP * LDV;
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const double y = acc[nt][i] - acc2[nt][i];
+        if (orow_ok) W[orow * LDV + 8 * nt + 2 * tq + i] = y;
+        if (oact[nt][i]) po[obase[nt][i] + (size_t)ev * ostep] = y;
+      }
+  };
+  __syncthreads();
+  // ------------------------------------------------------------ forward
+  double fa[KT], fc[KT], na[KT], nc[KT];
+#pragma unroll
+  for (int j = 0; j < D; ++j) issue_fwd(j);
+  frag(blk, fa);
+  frag(blk + MAT, fc);
+  cp_async_wait<D - 1>();
+  combine_fwd(0, 0);
+  __syncthreads();
+  for (int ev = 0; ev < KV; ++ev) {
+    const int buf = ev & 1;
+    issue_fwd(ev + D);
+    if (ev + 1 < KV) {
+      frag(blk + (size_t)(ev + 1) * 4 * MAT, na);
+      frag(blk + (size_t)(ev + 1) * 4 * MAT + MAT, nc);
+    }
+    step(buf, fa, fc, ev);
+    if (ev + 1 < KV) {
+      cp_async_wait<D - 1>();
+      combine_fwd(ev + 1, buf ^ 1);
+    }
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt) { fa[kt] = na[kt]; fc[kt] = nc[kt]; }
+    __syncthreads();
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  // ----------------------------------------------------------- backward
+  // step t uses buffer parity (KV + t) & 1; x_{KV} = 0
+  for (int i = threadIdx.x; i < KP * LDV; i += NTH) Wb[((KV & 1) ^ 1) * KP * LDV + i] = 0.0;
+#pragma unroll
+  for (int j = 0; j < D; ++j) issue_bwd(KV - 1 - j);
+  frag(blk + (size_t)(KV - 1) * 4 * MAT + 2 * MAT, fa);
+  frag(blk + (size_t)(KV - 1) * 4 * MAT + 3 * MAT, fc);
+  cp_async_wait<D - 1>();
+  combine_bwd(KV - 1, KV & 1);
+  __syncthreads();
+  for (int t = 0; t < KV; ++t) {
+    const int ev = KV - 1 - t;
+    const int buf = (KV + t) & 1;
+    issue_bwd(ev - D);
+    if (ev > 0) {
+      frag(blk + (size_t)(ev - 1) * 4 * MAT + 2 * MAT, na);
+      frag(blk + (size_t)(ev - 1) * 4 * MAT + 3 * MAT, nc);
+    }
+    step(buf, fa, fc, ev);
+    if (ev > 0) {
+      cp_async_wait<D - 1>();
+      combine_bwd(ev - 1, buf ^ 1);
+    }
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt) { fa[kt] = na[kt]; fc[kt] = nc[kt]; }
+    __syncthreads();
+  }
+  cp_async_wait<0>();
+}
+
+template <int NQ, int NS>
+void mma_launch(const BandSolve& B, cudaStream_t st) {
+  constexpr int BW1 = NQ * NS;
+  constexpr int NT = 2;
+  constexpr int D = 3;
+  constexpr int KP = 4 * ((BW1 + 3) / 4);
+  constexpr int LPC = 8 * NT;
+  constexpr int NTH = 32 * ((BW1 + 7) / 8);
+  static_assert(NQ * LPC <= NTH, "the right-hand-side loader needs NQ*LPC threads");
+  constexpr size_t smem = sizeof(double) * (4 * KP * (LPC + 4) + D * 5 * NS * NQ * LPC);
+  static bool configured = false;
+  if (!configured && smem > 48 * 1024)
+    cudaFuncSetAttribute(band_solve_mma_kernel<NQ, NS, NT, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+  configured = true;
+  band_solve_mma_kernel<NQ, NS, NT, D><<<(B.M.nlines + LPC - 1) / LPC, NTH, smem, st>>>(B, B.blk);
+}
+
+template <int NS> solve_fn pick_mma(int nq) {
+  switch (nq) {
+    case 2: return mma_launch<2, NS>;
+    case 3: return mma_launch<3, NS>;
+    case 4: return mma_launch<4, NS>;
+    case 5: return mma_launch<5, NS>;
+    case 6: return mma_launch<6, NS>;
+    case 7: return mma_launch<7, NS>;
+    case 8: return mma_launch<8, NS>;
+  }
+  return nullptr;
+}
+
 template <int NS> solve_fn pick_block(int nq) {
   switch (nq) {
     case 2: return block_launch<2, NS>;
@@ -384,9 +769,9 @@ void launch_block_prep(const double* band, int KV, int BW1, double* blk, cudaStr
 void launch_band_solve(const BandSolve& B, cudaStream_t st) {
   solve_fn f = nullptr;
   if (B.ld == 1 && B.blk) {
-    if (B.M.ns == 1) f = pick_block<1>(B.M.Nq);
-    if (B.M.ns == 4) f = pick_block<4>(B.M.Nq);
-    if (B.M.ns == 5) f = pick_block<5>(B.M.Nq);
+    if (B.M.ns == 1) f = pick_rows<1>(B.M.Nq);
+    if (B.M.ns == 4) f = pick_mma<4>(B.M.Nq);
+    if (B.M.ns == 5) f = pick_mma<5>(B.M.Nq);
   }
   if (!f && B.ld == 1) {
     if (B.M.ns == 1) f = pick_nq<1>(B.M.Nq);

@@ -33,6 +33,12 @@
 //   EPI_SUBOUT2  out = T; out2 -= T              (ARK, split_rhs = false:
 //                                                 im_K = L(Q), ex_K -= im_K)
 //   EPI_RLSRK    out = T; out2 = a*out2 + T      (relaxation LSRK: k, dq)
+//   EPI_ARK      IMEX stage of ARK23 with split_rhs = false, T = L(Q): with
+//                E = out - T (explicit part, out holding N(Q)) and I = T,
+//                every active accumulator j gets
+//                acc_j = (accin_j or Q) + adt*(ca_j*E + cb_j*I)
+//                -- the stage right-hand sides and the final update are
+//                accumulated here, so E and I are never stored
 #pragma once
 #include "atb_physics.cuh"
 
@@ -41,7 +47,7 @@ namespace atb {
 // VK_EC32: the entropy-conservative volume flux in the FP32-flux precision
 // form (mixed: balance-critical terms in FP64 adds/multiplies, the rest FP32)
 enum { VK_WEAK = 0, VK_CENTRAL = 1, VK_EC = 2, VK_KG = 3, VK_EC32 = 4 };
-enum { EPI_SET = 0, EPI_ADD = 1, EPI_LSRK = 2, EPI_SUBOUT2 = 3, EPI_RLSRK = 4 };
+enum { EPI_SET = 0, EPI_ADD = 1, EPI_LSRK = 2, EPI_SUBOUT2 = 3, EPI_RLSRK = 4, EPI_ARK = 5 };
 
 // neighbour-table encoding: relative offsets for interior faces, so an
 // instance's rows move between element ranges unchanged; NBR_BOUNDARY + tag
@@ -58,6 +64,10 @@ struct TendArgs {
   int dirs, sflux, epi;
   double a, bdt;
   const double* dte;  // per-element time step (batched instances), or null
+  // EPI_ARK accumulators (acc[j][0] null: inactive; accin[j][0] null: base Q)
+  double* acc[3][5];
+  const double* accin[3][5];
+  double ca[3], cb[3], adt;
   size_t stride;      // K*Np
   const double* q[5];
   double* out[5];
@@ -588,6 +598,18 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
         A.out2[s][gid] = qn[s] + bdt * dqn;
       }
     } break;
+    case EPI_ARK:
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const double E = A.out[s][gid] - T[s], I = T[s];
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          if (A.acc[j][0]) {
+            const double base = A.accin[j][0] ? A.accin[j][s][gid] : qn[s];
+            A.acc[j][s][gid] = base + A.adt * (A.ca[j] * E + A.cb[j] * I);
+          }
+      }
+      break;
     case EPI_SUBOUT2:
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
