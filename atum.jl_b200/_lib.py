@@ -70,6 +70,7 @@ SIGNATURES = {
     "atb_solver_set_dt": [_VP, C.c_double],
     "atb_solver_set_instance_dt": [_VP, _DP],
     "atb_solver_set_element_dt": [_VP, _DP],
+    "atb_solver_fuse": [_VP, C.c_int],
     "atb_weightednorm": [_VP, PtrArr, C.c_double, _DP, _DP, _VP],
     "atb_entropyintegral": [_VP, PtrArr, _DP, _VP],
     "atb_entropyproduct": [_VP, PtrArr, PtrArr, _DP, _VP],

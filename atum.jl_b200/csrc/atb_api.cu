@@ -195,6 +195,10 @@ void fill_args(const atb_op* op, TendArgs& A) {
     A.ca[j] = A.cb[j] = 0.0;
   }
   A.adt = 0.0;
+  A.lin_law = LawP{};
+  A.lin_sflux = 0;
+  A.lin_dirs = 0;
+  A.naux_nl = op->naux_used;
 }
 
 // EPI_ARK accumulators of one stage (see atb_tendency.cuh)
@@ -867,6 +871,10 @@ struct atb_solver {
   double* band = nullptr;
   double* blk = nullptr;
   int ld = 0;
+  // ARK23 stages fused into one kernel per stage (explicit tendency + linear
+  // operator), when the two operators allow it (atb_solver_fuse)
+  tend_launch_fn fused = nullptr;
+  bool fuse_on = false;
   // per-element time steps (LSRK over packed instances), or null; owned by
   // the solver (atb_solver_set_instance_dt) or by the caller
   double* d_dte = nullptr;
@@ -1138,6 +1146,51 @@ int rlsrk_step(atb_solver* s, double* const* q, cudaStream_t st) {
 // no stage tendency is ever stored, the banded solve reads one ready
 // right-hand side, and no separate combination kernel runs.  The additions
 // happen in the same order as in ark_step, so the results are identical.
+// one fused ARK stage launch: explicit tendency and linear operator of Q in
+// one pass, EPI_ARK accumulation (atb_tendency.cuh, FUSE = true)
+int run_fused(atb_solver* s, double* const* Q, const ArkAcc& ark, cudaStream_t st) {
+  atb_op* op = s->rhs;
+  TendArgs A;
+  fill_args(op, A);
+  const int naux = op->dim + 3;  // [Phi, grad Phi, rho_ref, p_ref] staged for both operators
+  A.naux = naux;
+  int E = op->E;
+  auto bytes = [&](int e) {
+    return tend_smem_bytes(op->ns, op->npre, naux, op->dim, op->Nq, op->Np, op->Nfp, e, op->npv, true);
+  };
+  // fused kernels are compiled for fused_max_threads per CTA
+  const int maxthr = fused_max_threads(op->Nq);
+  while (E > 1 && (E * op->Np > maxthr || bytes(E) > 100 * 1024)) --E;
+  if (E * op->Np > maxthr) return fail(ATB_ERR_INVALID, "element too large for the fused ARK stage kernel");
+  A.E = E;
+  A.epi = EPI_ARK;
+  A.lin_law = s->lin->law;
+  A.lin_sflux = s->lin->sflux;
+  A.lin_dirs = s->lin->dirs;
+  for (int j = 0; j < 3; ++j) {
+    for (int c = 0; c < 5; ++c) { A.acc[j][c] = ark.acc[j][c]; A.accin[j][c] = ark.accin[j][c]; }
+    A.ca[j] = ark.ca[j];
+    A.cb[j] = ark.cb[j];
+  }
+  A.adt = ark.adt;
+  for (int c = 0; c < 5; ++c) {
+    A.q[c] = Q[c];
+    A.out[c] = Q[c];  // not read by the fused epilogue
+    A.out2[c] = nullptr;
+  }
+  const int grid = (op->K_active + E - 1) / E;
+  if (grid == 0) return ATB_OK;
+  {
+    ProfScope ps(ATB_PROF_TEND, st);
+    s->fused(A, grid, E * op->Np, bytes(E), st);
+  }
+  const cudaError_t le = cudaGetLastError();
+  if (le != cudaSuccess)
+    return fail(ATB_ERR_CUDA, "fused ARK stage launch (%d elements of %d nodes per CTA, %zu bytes of shared memory): %s",
+                E, op->Np, bytes(E), cudaGetErrorString(le));
+  return ATB_OK;
+}
+
 int ark_step_accumulated(atb_solver* s, double* const* q, cudaStream_t st) {
   const int ns = s->ns;
   const size_t n = s->stride;
@@ -1181,29 +1234,33 @@ int ark_step_accumulated(atb_solver* s, double* const* q, cudaStream_t st) {
   };
   int rc;
   ArkAcc a;
+  // one stage: N(Q) then L(Q) with the accumulation, or both in one launch
+  auto stage = [&](double* const* Q) -> int {
+    if (s->fuse_on) return run_fused(s, Q, a, st);
+    int r;
+    if ((r = run_tendency(s->rhs, EPI_SET, Q, N, nullptr, 0, 0, st))) return r;
+    return run_tendency(s->lin, EPI_ARK, Q, N, nullptr, 0, 0, st, nullptr, &a);
+  };
   // stage 1 (Q = q): R1, R2, F from q
-  if ((rc = run_tendency(s->rhs, EPI_SET, qq, N, nullptr, 0, 0, st))) return rc;
   acc_clear(a);
   a.adt = s->dt;
   set(a, 0, R1, nullptr, s->exa[1][0], s->ima[1][0]);
   set(a, 1, R2, nullptr, s->exa[2][0], s->ima[2][0]);
   set(a, 2, F, nullptr, s->exb[0], s->imb[0]);
-  if ((rc = run_tendency(s->lin, EPI_ARK, qq, N, nullptr, 0, 0, st, nullptr, &a))) return rc;
+  if ((rc = stage(qq))) return rc;
   // stage 2
   if ((rc = solve(R1, Q1))) return rc;
-  if ((rc = run_tendency(s->rhs, EPI_SET, Q1, N, nullptr, 0, 0, st))) return rc;
   acc_clear(a);
   a.adt = s->dt;
   set(a, 0, R2, R2, s->exa[2][1], s->ima[2][1]);
   set(a, 1, F, F, s->exb[1], s->imb[1]);
-  if ((rc = run_tendency(s->lin, EPI_ARK, Q1, N, nullptr, 0, 0, st, nullptr, &a))) return rc;
+  if ((rc = stage(Q1))) return rc;
   // stage 3 and the update of q
   if ((rc = solve(R2, Q2))) return rc;
-  if ((rc = run_tendency(s->rhs, EPI_SET, Q2, N, nullptr, 0, 0, st))) return rc;
   acc_clear(a);
   a.adt = s->dt;
   set(a, 0, qq, F, s->exb[2], s->imb[2]);
-  if ((rc = run_tendency(s->lin, EPI_ARK, Q2, N, nullptr, 0, 0, st, nullptr, &a))) return rc;
+  if ((rc = stage(Q2))) return rc;
   s->time += s->dt;
   return ATB_OK;
 }
@@ -1311,6 +1368,8 @@ int do_steps(atb_solver* s, double* const* q, int nsteps, cudaStream_t st) {
 
 }  // namespace
 
+int fusion_check(atb_solver* s, cudaStream_t st);
+
 extern "C" int atb_solver_create(int kind, atb_op* rhs, atb_op* linrhs, double dt, double t0, int split_rhs,
                                  int paperversion, atb_solver** out) {
   if (!out) return fail(ATB_ERR_INVALID, "null argument");
@@ -1370,6 +1429,11 @@ extern "C" int atb_solver_create(int kind, atb_op* rhs, atb_op* linrhs, double d
       solver_free(s);
       return rc;
     }
+    if ((rc = fusion_check(s, 0))) {
+      solver_free(s);
+      return rc;
+    }
+    s->fuse_on = s->fused != nullptr;
   }
   if ((rc = check_launch("solver create"))) { solver_free(s); return rc; }
   *out = s;
@@ -1419,6 +1483,48 @@ extern "C" int atb_solver_set_dt(atb_solver* s, double dt) {
   if (s->kind == ATB_ARK23 && s->lin && dt != s->dt)
     return fail(ATB_ERR_INVALID, "ARK23 factors I - dt a L for a fixed dt");
   s->dt = dt;
+  return ATB_OK;
+}
+
+// Can the explicit and the linear operator of this ARK23 solver run as one
+// kernel per stage?  Euler-gravity (3-D, EC or FP32-flux EC volume flux) with
+// the weak-form linear Euler-gravity operator along z only, on the same grid
+// (bitwise identical metrics and neighbours) with the same leading aux fields
+// [Phi, grad Phi, rho_ref, p_ref] (bitwise identical on the device).
+int fusion_check(atb_solver* s, cudaStream_t st) {
+  s->fused = nullptr;
+  atb_op *R = s->rhs, *L = s->lin;
+  if (s->kind != ATB_ARK23 || !R || !L || s->split_rhs || !s->band) return ATB_OK;
+  if (R->law.kind != LAW_EG || L->law.kind != LAW_LEG || R->dim != 3 || L->vk != VK_WEAK) return ATB_OK;
+  if (L->dirs != (1 << (R->dim - 1))) return ATB_OK;
+  if (R->K != L->K || R->Np != L->Np || R->stacked != L->stacked) return ATB_OK;
+  const int na = R->dim + 3;
+  if (R->naux < na || L->naux < na) return ATB_OK;
+  tend_launch_fn f = pick_launcher_fused(R->dim, R->vk, R->Nq);
+  if (!f) return ATB_OK;
+  unsigned long long* d_cnt = nullptr;
+  int rc;
+  if ((rc = dalloc(&d_cnt, 1))) return rc;
+  CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st));
+  const size_t K = (size_t)R->K, n = R->stride();
+  launch_count_diff(R->d_ginv, L->d_ginv, K * 3 * 2, d_cnt, st);
+  launch_count_diff(R->d_J, L->d_J, K * 2, d_cnt, st);
+  launch_count_diff(R->d_nbr, L->d_nbr, K * 6, d_cnt, st);
+  for (int k = 0; k < na; ++k) launch_count_diff(R->d_aux + (size_t)k * n, L->d_aux + (size_t)k * n, n * 2, d_cnt, st);
+  unsigned long long cnt = 1;
+  cudaError_t e1 = cudaMemcpyAsync(&cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, st);
+  cudaError_t e2 = cudaStreamSynchronize(st);
+  cudaFree(d_cnt);
+  if (e1 != cudaSuccess || e2 != cudaSuccess) return fail(ATB_ERR_CUDA, "fusion check failed");
+  if (cnt == 0) s->fused = f;
+  return ATB_OK;
+}
+
+extern "C" int atb_solver_fuse(atb_solver* s, int enable) {
+  if (!s) return fail(ATB_ERR_INVALID, "null solver");
+  if (enable && !s->fused)
+    return fail(ATB_ERR_INVALID, "this solver's operators cannot run as one kernel per stage");
+  s->fuse_on = enable && s->fused;
   return ATB_OK;
 }
 

@@ -45,6 +45,17 @@ __global__ void axpy_kernel(const Axpy A) {
 
 void launch_axpy(const Axpy& A, cudaStream_t st) { axpy_kernel<<<grid_for(A.n, 256), 256, 0, st>>>(A); }
 
+__global__ void count_diff_kernel(const unsigned* a, const unsigned* b, size_t n, unsigned long long* count) {
+  unsigned long long c = 0;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) c += (a[i] != b[i]);
+  if (c) atomicAdd(count, c);
+}
+
+void launch_count_diff(const void* a, const void* b, size_t nwords, unsigned long long* count, cudaStream_t st) {
+  count_diff_kernel<<<grid_for(nwords, 256), 256, 0, st>>>((const unsigned*)a, (const unsigned*)b, nwords, count);
+}
+
 // ------------------------------------------------------------ band probe
 __device__ __forceinline__ size_t line_gid(const LineMap& M, int line, int ev, int kv) {
   const int eh = line / M.nh, hn = line - eh * M.nh;

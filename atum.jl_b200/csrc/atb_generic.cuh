@@ -32,6 +32,8 @@ struct Axpy {
   double* out[5];
 };
 void launch_axpy(const Axpy& A, cudaStream_t st);
+// number of differing 32-bit words of two device arrays, added to *count
+void launch_count_diff(const void* a, const void* b, size_t nwords, unsigned long long* count, cudaStream_t st);
 
 // Vertical lines of nodes: line l = eh * nh + hn (horizontal element stack eh,
 // horizontal node hn); unknown u = (ev * Nq + kv) * ns + s.

@@ -68,6 +68,11 @@ struct TendArgs {
   double* acc[3][5];
   const double* accin[3][5];
   double ca[3], cb[3], adt;
+  // fused linear operator (tendency_kernel<..., FUSE = true>): the linear
+  // Euler-gravity law, its surface flux and directions
+  LawP lin_law;
+  int lin_sflux, lin_dirs;
+  int naux_nl;  // aux components the explicit operator's faces read (fused launches stage more)
   size_t stride;      // K*Np
   const double* q[5];
   double* out[5];
@@ -102,10 +107,12 @@ template <int LAW, int DIM, int VK> struct NPairVals {
   static constexpr int stride = v | 1;
 };
 
-inline size_t tend_smem_bytes(int ns, int npre, int naux, int dim, int Nq, int Np, int Nfp, int E, int npvs) {
+inline size_t tend_smem_bytes(int ns, int npre, int naux, int dim, int Nq, int Np, int Nfp, int E, int npvs,
+                              bool fuse = false) {
   const int npl = Nq * (Nq - 1) / 2;
   size_t per = (size_t)(ns + naux + npre) * Np + (size_t)2 * dim * Nfp * ns;
   if (npvs > 0) per += (size_t)Nfp * npl * npvs;
+  if (fuse) per += (size_t)ns * Np + (size_t)2 * Nfp * ns;  // linear flux rows, linear face slots
   return sizeof(double) * (2 * (size_t)Nq * Nq + 2 + per * E) + 64 * sizeof(int);
 }
 
@@ -267,11 +274,10 @@ __device__ __forceinline__ int pair_index(int a, int b, int Nq) { return a * Nq 
 // the neighbour trace (or the boundary state), evaluate the numerical flux and
 // store it lifted into the face's shared-memory slot
 template <int LAW, int DIM, int NAM, int D_>
-__device__ __forceinline__ void face_task(const TendArgs& A, const LawP& L, int Nq, int Np, int Nfp, int e, int t,
-                                          const double* sq, const double* sa, double* ss, double gid,
-                                          double lift_end) {
+__device__ __forceinline__ void face_task(const TendArgs& A, const LawP& L, int sflux, int naux, int Nq, int Np,
+                                          int Nfp, int e, int t, const double* sq, const double* sa, double* ss,
+                                          double gid, double lift_end) {
   constexpr int NS = NSt<LAW, DIM>::v;
-  const int naux = A.naux;
   const int face = t / Nfp, j = t - face * Nfp;
   const int side = face & 1;
   if (!((A.dirs >> D_) & 1)) return;
@@ -302,7 +308,7 @@ __device__ __forceinline__ void face_task(const TendArgs& A, const LawP& L, int 
     for (int k = 0; k < NAM; ++k) ap[k] = am[k];
   }
   double nf[NS];
-  surface_flux<LAW, DIM>(L, A.sflux, D_, sgn, qm, am, qp, ap, nf);
+  surface_flux<LAW, DIM>(L, sflux, D_, sgn, qm, am, qp, ap, nf);
   const double lift = gid * lift_end;
 #pragma unroll
   for (int s = 0; s < NS; ++s) ss[(face * Nfp + j) * NS + s] = lift * nf[s];
@@ -310,8 +316,17 @@ __device__ __forceinline__ void face_task(const TendArgs& A, const LawP& L, int 
 
 // NQ_ > 0: the node count per direction is a compile-time constant (index
 // arithmetic folds, line loops unroll); NQ_ = 0 reads it from the arguments.
-template <int LAW, int DIM, int VK, int NQ_>
-__global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
+// CTA size limit of the fused kernels: 256 threads unless one element needs
+// more
+__host__ __device__ constexpr int fused_max_threads(int nq) { return (nq == 0 || nq * nq * nq > 256) ? 512 : 256; }
+
+// Plain launches: up to 512 threads.  Fused launches (which carry the linear
+// operator too): fused_max_threads, with enough resident CTAs requested that
+// the register budget stays at 128 -- measured faster on B200 than the
+// spill-free 156-register allocation, whose lower occupancy costs more.
+template <int LAW, int DIM, int VK, int NQ_, bool FUSE = false>
+__global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 512 / fused_max_threads(NQ_) : 1)
+    tendency_kernel(const TendArgs A) {
   constexpr int NS = NSt<LAW, DIM>::v;
   constexpr int NPRE = NPre<LAW, DIM, VK>::v;
   constexpr int NAM = NAuxMax<LAW, DIM>::v;
@@ -333,12 +348,15 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
   const int tabn = 2 * Nq * Nq + 2;
   double* sC = sm;            // Cfd
   double* sW = sm + Nq * Nq;  // Cw
-  const size_t slotsz = (size_t)(NS + naux + NPRE) * Np + (size_t)2 * DIM * Nfp * NS + (size_t)Nfp * npl * NPVS;
+  const size_t slotsz = (size_t)(NS + naux + NPRE) * Np + (size_t)2 * DIM * Nfp * NS + (size_t)Nfp * npl * NPVS +
+                        (FUSE ? (size_t)NS * Np + (size_t)2 * Nfp * NS : 0);
   double* sq = sm + tabn + slot * slotsz;
   double* sa = sq + NS * Np;
   double* sp = sa + naux * Np;
   double* ss = sp + NPRE * Np;
   double* spv = ss + 2 * DIM * Nfp * NS;  // pair values
+  double* slf = spv + (size_t)Nfp * npl * NPVS;  // FUSE: linear vertical flux per node
+  double* ssl = slf + NS * Np;                   // FUSE: linear z-face slots
   int* spair = (int*)(sm + tabn + A.E * slotsz);
   for (int t = threadIdx.x; t < tabn; t += blockDim.x) sm[t] = A.tab[t];
   if (PAIRS && threadIdx.x < npl) {
@@ -426,6 +444,16 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
 #pragma unroll
         for (int s = 0; s < NS; ++s) sp[(d * NS + s) * Np + node] = f[s];
       }
+    }
+  }
+  if constexpr (FUSE && LAW == LAW_EG) {
+    // fused linear operator: its z flux rows, staged with the state (no
+    // barrier of its own)
+    if (act) {
+      double f[NS];
+      flux_dir<LAW_LEG, DIM>(A.lin_law, DIM - 1, qn, an, f);
+#pragma unroll
+      for (int s = 0; s < NS; ++s) slf[s * Np + node] = f[s];
     }
   }
   __syncthreads();
@@ -550,17 +578,54 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
     }
   }
 
+  // ------------------------------------ fused linear operator (volume)
+  // the weak-form linear Euler-gravity operator along z, evaluated exactly as
+  // its own launch would: sources, then the D^T contraction of the staged
+  // flux rows, then (below) the z faces
+  constexpr int DZ = DIM - 1;
+  double TL[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) TL[s] = 0.0;
+  if constexpr (FUSE && LAW == LAW_EG) {
+    if (act && ((A.lin_dirs >> DZ) & 1)) {
+      add_sources<LAW_LEG, DIM>(A.lin_law, true, qn, an, TL);
+      const int sd = (DZ == 0) ? 1 : (DZ == 1) ? Nq : Nq * Nq;
+      const int id = ijk[DZ];
+      const int base = node - id * sd;
+#pragma unroll
+      for (int m = 0; m < (CQ ? NQ_ : 8); ++m) {
+        if (!CQ && m >= Nq) break;
+        const int nn = base + m * sd;
+        const double c = sW[id * Nq + m] * gi[DZ];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) TL[s] = TL[s] + c * slf[s * Np + nn];
+      }
+    }
+  }
+
   // ------------------------------------------------------------ faces
   // the face direction is dispatched to a compile-time constant so every
   // state / normal index in the numerical flux is static (no local memory)
   if (act) {
     const double lift_end = sm[2 * Nq * Nq];
-    for (int t = node; t < 2 * DIM * Nfp; t += Np) {
+    const int ntask = 2 * DIM * Nfp + ((FUSE && LAW == LAW_EG && ((A.lin_dirs >> DZ) & 1)) ? 2 * Nfp : 0);
+    const int naux_nl = FUSE ? A.naux_nl : naux;
+    for (int t = node; t < ntask; t += Np) {
+      if constexpr (FUSE && LAW == LAW_EG) {
+        if (t >= 2 * DIM * Nfp) {
+          // z faces of the linear operator (face numbers 2*DZ, 2*DZ + 1): the
+          // slot pointer is shifted so those faces land in the linear slots
+          face_task<LAW_LEG, DIM, NAuxMax<LAW_LEG, DIM>::v, DZ>(A, A.lin_law, A.lin_sflux, naux, Nq, Np, Nfp, e,
+                                                                 t - 2 * DIM * Nfp + 2 * DZ * Nfp, sq, sa,
+                                                                 ssl - (size_t)2 * DZ * Nfp * NS, gi[DZ], lift_end);
+          continue;
+        }
+      }
       const int face = t / Nfp;
       switch (face >> 1) {
-        case 0: face_task<LAW, DIM, NAM, 0>(A, L, Nq, Np, Nfp, e, t, sq, sa, ss, gi[0], lift_end); break;
-        case 1: if constexpr (DIM > 1) face_task<LAW, DIM, NAM, 1>(A, L, Nq, Np, Nfp, e, t, sq, sa, ss, gi[1], lift_end); break;
-        default: if constexpr (DIM > 2) face_task<LAW, DIM, NAM, 2>(A, L, Nq, Np, Nfp, e, t, sq, sa, ss, gi[2], lift_end); break;
+        case 0: face_task<LAW, DIM, NAM, 0>(A, L, A.sflux, naux_nl, Nq, Np, Nfp, e, t, sq, sa, ss, gi[0], lift_end); break;
+        case 1: if constexpr (DIM > 1) face_task<LAW, DIM, NAM, 1>(A, L, A.sflux, naux_nl, Nq, Np, Nfp, e, t, sq, sa, ss, gi[1], lift_end); break;
+        default: if constexpr (DIM > 2) face_task<LAW, DIM, NAM, 2>(A, L, A.sflux, naux_nl, Nq, Np, Nfp, e, t, sq, sa, ss, gi[2], lift_end); break;
       }
     }
   }
@@ -575,6 +640,15 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
     const int j = (d == 0) ? ijk[1] + Nq * ijk[2] : (d == 1) ? ijk[0] + Nq * ijk[2] : ijk[0] + Nq * ijk[1];
 #pragma unroll
     for (int s = 0; s < NS; ++s) T[s] = T[s] - ss[(face * Nfp + j) * NS + s];
+  }
+  if constexpr (FUSE && LAW == LAW_EG) {
+    const int id = ijk[DZ];
+    if (((A.lin_dirs >> DZ) & 1) && (id == 0 || id == Nq - 1)) {
+      const int side = (id == Nq - 1) ? 1 : 0;
+      const int j = (DZ == 0) ? ijk[1] + Nq * ijk[2] : (DZ == 1) ? ijk[0] + Nq * ijk[2] : ijk[0] + Nq * ijk[1];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) TL[s] = TL[s] - ssl[(side * Nfp + j) * NS + s];
+    }
   }
 
   // --------------------------------------------------------- epilogue
@@ -601,7 +675,9 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
     case EPI_ARK:
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
-        const double E = A.out[s][gid] - T[s], I = T[s];
+        // fused: T = N(Q), TL = L(Q); else out holds N(Q) and T = L(Q)
+        const double E = FUSE ? T[s] - TL[s] : A.out[s][gid] - T[s];
+        const double I = FUSE ? TL[s] : T[s];
 #pragma unroll
         for (int j = 0; j < 3; ++j)
           if (A.acc[j][0]) {
@@ -630,15 +706,22 @@ __global__ void __launch_bounds__(512) tendency_kernel(const TendArgs A) {
 // launcher signature used by the host dispatch table
 typedef void (*tend_launch_fn)(const TendArgs& A, int grid, int block, size_t smem, cudaStream_t st);
 
-template <int LAW, int DIM, int VK, int NQ_ = 0>
+template <int LAW, int DIM, int VK, int NQ_ = 0, bool FUSE = false>
 void tend_launch(const TendArgs& A, int grid, int block, size_t smem, cudaStream_t st) {
   static size_t configured = 0;
   if (smem > 48 * 1024 && smem > configured) {
-    cudaFuncSetAttribute(tendency_kernel<LAW, DIM, VK, NQ_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    configured = smem;
+    // on failure the launch below reports the error
+    if (cudaFuncSetAttribute(tendency_kernel<LAW, DIM, VK, NQ_, FUSE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) == cudaSuccess)
+      configured = smem;
   }
-  tendency_kernel<LAW, DIM, VK, NQ_><<<grid, block, smem, st>>>(A);
+  tendency_kernel<LAW, DIM, VK, NQ_, FUSE><<<grid, block, smem, st>>>(A);
 }
+
+// Euler-gravity explicit tendency fused with the weak-form linear operator
+// along z (ARK23 stages, split_rhs = false): 3-D, EC / FP32-flux EC volume
+// flux; nullptr when there is no such kernel
+tend_launch_fn pick_launcher_fused(int dim, int vk, int nq);
 
 // generic (runtime Nq) launcher, and the compile-time-Nq specialisations
 // that exist for (law, dim, vk, nq) -- nullptr when there is none

@@ -64,6 +64,11 @@ class Solver:
     def gamma(self) -> float:
         return self._get()[2]
 
+    def fuse(self, enable: bool = True):
+        """ARK23: run the explicit and the linear operator of a stage as one
+        kernel (on by default when the operators allow it)."""
+        _lib.check(_lib.lib().atb_solver_fuse(self.h, int(bool(enable))))
+
     def step(self, q, nsteps: int = 1, stream=None):
         """``dostep!`` repeated ``nsteps`` times (no host synchronisation)."""
         _lib.check(_lib.lib().atb_solver_step(self.h, _lib.field_ptrs(q, self.ns), int(nsteps),

@@ -185,6 +185,13 @@ int atb_solver_set_dt(atb_solver* s, double dt);
  * doubles), read by every later stage, so its contents may change between
  * steps without another call; NULL returns to the single dt. */
 int atb_solver_set_instance_dt(atb_solver* s, const double* dt_host);
+/* ARK23 kernel fusion (no reference counterpart): when the explicit operator is
+ * 3-D Euler-gravity with an EC / FP32-flux EC volume flux and the implicit one
+ * the weak-form linear Euler-gravity operator along z on the same grid and aux
+ * fields (split_rhs = false), each stage runs both as one kernel; on by
+ * default when possible.  enable = 0 runs them as two launches; enabling a
+ * solver that cannot fuse is an error. */
+int atb_solver_fuse(atb_solver* s, int enable);
 int atb_solver_set_element_dt(atb_solver* s, const double* dte_device);
 
 /* measures -- src/measures.jl:6-33 (p = 2 or INFINITY); results to host memory */
