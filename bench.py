@@ -39,7 +39,8 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 # Algorithmic FP64 flops per DOF-stage of the flux-differencing tendency
 # (EC volume flux, Rusanov surface flux), from the oracle's instrumented
 # counter: python oracle/count_flops.py
-FLOPS_PER_DOF_STAGE = {"bubble_3d_N4_ec_rusanov": 602.8, "bubble_3d_N7_ec_rusanov": 896.2}
+FLOPS_PER_DOF_STAGE = {"bubble_3d_N4_ec_rusanov": 602.8, "bubble_3d_N7_ec_rusanov": 896.2,
+                       "bubble_3d_N4_linear_weak_z": 22.4, "bubble_3d_N7_linear_weak_z": 25.1}
 L2_BYTES = 126 * 2 ** 20
 
 
@@ -244,8 +245,6 @@ def run_ours(args):
     barrier()
     n0 = _lib.C.c_long()
     L.atb_launch_count(_lib.C.byref(n0))
-    _lib.check(L.atb_profile_reset())
-    _lib.check(L.atb_profile_enable(1))
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(torch.cuda.current_device()) as clk:
         barrier()
@@ -253,11 +252,18 @@ def run_ours(args):
         solver.step(q, args.steps)
         ev1.record(stream)
         barrier()
-    _lib.check(L.atb_profile_enable(0))
     ms = ev0.elapsed_time(ev1)
     n1 = _lib.C.c_long()
     L.atb_launch_count(_lib.C.byref(n1))
-    prof = {}
+    # per-kernel times from a second pass with the library's per-launch CUDA
+    # events (kept out of the headline timing above)
+    kprof = max(3, min(args.steps, 30))
+    _lib.check(L.atb_profile_reset())
+    _lib.check(L.atb_profile_enable(1))
+    solver.step(q, kprof)
+    barrier()
+    _lib.check(L.atb_profile_enable(0))
+    prof = {"steps": kprof}
     for k, name in enumerate(("tendency", "tendency_linear", "band_solve", "combine", "reduce")):
         nl, tm = _lib.C.c_long(), _lib.C.c_double()
         _lib.check(L.atb_profile_read(k, _lib.C.byref(nl), _lib.C.byref(tm)))
@@ -303,15 +309,22 @@ def run_ours(args):
     e2e = world * dofs * 3 * ke / (ms_e2e * 1e-3)
     tend = prof["tendency"]
     avg_ms = tend["ms"] / max(1, tend["launches"])
-    key = "bubble_3d_N4_ec_rusanov"
-    flops_launch = FLOPS_PER_DOF_STAGE[key] * dofs
+    # the stage kernel: explicit EC tendency fused with the linear vertical
+    # operator when the solver fuses them (no separate linear launches)
+    fused = prof["tendency_linear"]["launches"] == 0
+    flops_dof = FLOPS_PER_DOF_STAGE["bubble_3d_N4_ec_rusanov"]
+    if fused:
+        flops_dof += FLOPS_PER_DOF_STAGE["bubble_3d_N4_linear_weak_z"]
+    flops_launch = flops_dof * dofs
     tflops = flops_launch / (avg_ms * 1e-3) / 1e12
     peak_fp64 = _lib.C.c_double()
     _lib.check(L.atb_probe_fp64_peak(_lib.C.byref(peak_fp64), _lib.stream_ptr()))
     peaks, kind = measured_peaks()
-    # algorithmic bytes of the fused FP64 tendency launch: q (5 values) read,
-    # ex_K (5) written, Phi (1) read = 11 x 8 B per node
-    bytes_launch = 11 * 8 * dofs // 5
+    # algorithmic bytes per launch: fused stage kernel, averaged over the three
+    # stages: Q (5) and aux (6) read; accumulators 15 written (stage 1), 10 read
+    # + 10 written (stage 2), 5 read + 5 written (stage 3) -> 26 x 8 B per node.
+    # Unfused explicit tendency: Q (5), Phi (1) read, N(Q) (5) written.
+    bytes_launch = (26 if fused else 11) * 8 * dofs // 5
     line = {
         "metric": "DOF-stage updates/s", "value": value, "unit": "DOF-stage/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -326,14 +339,19 @@ def run_ours(args):
         "e2e": {"value": e2e, "unit": "DOF-stage/s", "h2d_bytes_per_step": dofs * 8, "d2h_bytes_per_step": dofs * 8,
                 "steps": ke},
         "gpu_launches": int(n1.value - n0.value),
-        "roofline": {"bound": "fp64", "kernel": "tendency_kernel<EulerGravity,3,EC> (nonlinear stage tendency)",
+        "roofline": {"bound": "fp64",
+                     "kernel": ("tendency_kernel<EulerGravity,3,EC,Nq=5,fused> (ARK23 stage: EC tendency + linear "
+                                "vertical operator)") if fused else
+                               "tendency_kernel<EulerGravity,3,EC,Nq=5> (explicit stage tendency)",
+                     "flops_per_dof_stage": flops_dof,
                      "achieved": tflops, "peak": peak_fp64.value, "unit": "TFLOP/s",
                      "frac": tflops / peak_fp64.value if peak_fp64.value > 0 else None,
                      "peak_source": "measured in this run: FP64 FMA probe (atb_probe_fp64_peak)",
                      "flops_per_launch": flops_launch, "avg_launch_ms": avg_ms,
-                     "traffic": profiled_traffic() if args.precision == "fp64" else None,
+                     "traffic": profiled_traffic(PROFILE_FUSED if fused else PROFILE_TEND)
+                     if args.precision == "fp64" else None,
                      "traffic_unit": "bytes per launch (dram read + write, one ncu capture)",
-                     "traffic_source": PROFILE_TEND,
+                     "traffic_source": PROFILE_FUSED if fused else PROFILE_TEND,
                      "hbm_view": {"bytes_per_launch": bytes_launch,
                                   "achieved_gbs": bytes_launch / (avg_ms * 1e-3) / 1e9,
                                   "peak_gbs": peaks["hbm_gbs"], "peak_kind": kind}},
@@ -349,6 +367,7 @@ def run_ours(args):
 
 
 PROFILE_TEND = "profiles/tendency_eg3_ec_nq5_bubble16.md"
+PROFILE_FUSED = "profiles/tendency_eg3_ec_nq5_fused_bubble16.md"
 
 
 # ------------------------------------------------------------ serving stream
@@ -585,10 +604,10 @@ def run_swbatch(args):
     return 0
 
 
-def profiled_traffic():
-    """DRAM bytes (read + write) of one FP64 tendency launch of this workload,
-    from the committed ncu summary of the same kernel and workload."""
-    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), PROFILE_TEND)
+def profiled_traffic(profile=PROFILE_TEND):
+    """DRAM bytes (read + write) of one FP64 launch of the kernel and workload
+    a committed ncu summary covers."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), profile)
     try:
         with open(path) as f:
             for ln in f:

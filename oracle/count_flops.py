@@ -40,6 +40,29 @@ def fd_flops(dg, vflux_kind, sflux_kind, q1, a1, q2, a2):
             "twopoint": tp, "surface": sf}
 
 
+def weak_flops(dg, sflux_kind, q1, a1, q2, a2):
+    """Weak-form operator restricted to its directions (the linear
+    Euler-gravity operator of the IMEX stages, directions = (dim,)): per node
+    the reference's full flux matrix, the D^T contraction of each active
+    direction (Nq multiply-adds per state), the law's source (2 per
+    dimension); per face node of each active direction's two faces one surface
+    flux; divided by Np*Ns."""
+    import pyoracle as orc
+    law = dg.law
+    dim, Nq = law.dim, dg.grid.cell.Nq
+    ns = law.numberofstates
+    nd = len(dg.directions)
+    n = [0.0] * 3
+    n[dg.directions[-1] - 1] = 1.0
+    fx = orc.count_flops(dg, 0, 0, q1, a1, q2, a2, n)
+    sf = orc.count_flops(dg, 2, sflux_kind, q1, a1, q2, a2, n)
+    f_fx = sum(fx[k] for k in ("add", "mul", "div", "sqrt", "log", "pow"))
+    f_sf = sum(sf[k] for k in ("add", "mul", "div", "sqrt", "log", "pow"))
+    Np = Nq ** dim
+    per_elem = Np * (f_fx + nd * 2 * Nq * ns + 2 * dim) + nd * 2 * Nq ** (dim - 1) * f_sf
+    return {"flops_per_dof_stage": per_elem / (Np * ns), "flux": fx, "surface": sf}
+
+
 def main():
     import problems as P
     out = {}
@@ -48,6 +71,7 @@ def main():
     a = case.dg.auxstate_host()
     q1, q2, a1, a2 = x[:, 0, 0], x[:, 1, 7], a[:, 0, 0], a[:, 1, 7]
     out["bubble_3d_N4_ec_rusanov"] = fd_flops(case.dg, 2, 1, q1, a1, q2, a2)
+    out["bubble_3d_N4_linear_weak_z"] = weak_flops(case.lindg, 1, q1, a1, q2, a2)
     c1 = P.vortex_c1()
     x = c1.q0
     out["vortex_2d_N3_ec_rusanov"] = fd_flops(c1.dg, 2, 1, x[:, 0, 0], [], x[:, 3, 5], [])
@@ -55,6 +79,7 @@ def main():
     x = c5.q0
     a = c5.dg.auxstate_host()
     out["bubble_3d_N7_ec_rusanov"] = fd_flops(c5.dg, 2, 1, x[:, 0, 0], a[:, 0, 0], x[:, 1, 9], a[:, 1, 9])
+    out["bubble_3d_N7_linear_weak_z"] = weak_flops(c5.lindg, 1, x[:, 0, 0], a[:, 0, 0], x[:, 1, 9], a[:, 1, 9])
     print(json.dumps(out, indent=1, sort_keys=True))
 
 
