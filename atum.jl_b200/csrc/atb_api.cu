@@ -168,6 +168,10 @@ struct atb_op {
 
 namespace {
 
+// CTA size of a tendency launch: E elements of Np nodes, rounded up to whole
+// warps (the face tasks are spread over warp-aligned groups)
+int cta_threads(int E, int Np) { return ((E * Np + 31) / 32) * 32; }
+
 size_t op_smem(const atb_op* op, int E) {
   return tend_smem_bytes(op->ns, op->npre, op->naux_used, op->dim, op->Nq, op->Np, op->Nfp, E, op->npv);
 }
@@ -234,7 +238,7 @@ int run_tendency(atb_op* op, int epi, const double* const* q, double* const* out
   if (grid == 0) return ATB_OK;
   {
     ProfScope ps(op->prof_class, st);
-    op->launch(A, grid, op->E * op->Np, op->smem, st);
+    op->launch(A, grid, cta_threads(op->E, op->Np), op->smem, st);
   }
   return check_launch("tendency");
 }
@@ -729,7 +733,7 @@ extern "C" int atb_op_autotune(atb_op* op, const double* const* q, double* scrat
   cudaEvent_t a, b;
   CK(cudaEventCreate(&a));
   CK(cudaEventCreate(&b));
-  for (int E = 1; E * op->Np <= 512 && E <= 16; ++E) {
+  for (int E = 1; cta_threads(E, op->Np) <= 512 && E <= 16; ++E) {
     if (op_smem(op, E) > 200 * 1024) break;
     op->E = E;
     op->smem = op_smem(op, E);
@@ -752,7 +756,8 @@ extern "C" int atb_op_autotune(atb_op* op, const double* const* q, double* scrat
 }
 
 extern "C" int atb_op_set_launch(atb_op* op, int elements_per_cta) {
-  if (!op || elements_per_cta < 1 || elements_per_cta * op->Np > 512 || op_smem(op, elements_per_cta) > 227 * 1024)
+  if (!op || elements_per_cta < 1 || cta_threads(elements_per_cta, op->Np) > 512 ||
+      op_smem(op, elements_per_cta) > 227 * 1024)
     return fail(ATB_ERR_INVALID, "bad elements per CTA");
   op->E = elements_per_cta;
   op->smem = op_smem(op, elements_per_cta);
@@ -1160,8 +1165,8 @@ int run_fused(atb_solver* s, double* const* Q, const ArkAcc& ark, cudaStream_t s
   };
   // fused kernels are compiled for fused_max_threads per CTA
   const int maxthr = fused_max_threads(op->Nq);
-  while (E > 1 && (E * op->Np > maxthr || bytes(E) > 100 * 1024)) --E;
-  if (E * op->Np > maxthr) return fail(ATB_ERR_INVALID, "element too large for the fused ARK stage kernel");
+  while (E > 1 && (cta_threads(E, op->Np) > maxthr || bytes(E) > 100 * 1024)) --E;
+  if (cta_threads(E, op->Np) > maxthr) return fail(ATB_ERR_INVALID, "element too large for the fused ARK stage kernel");
   A.E = E;
   A.epi = EPI_ARK;
   A.lin_law = s->lin->law;
@@ -1182,7 +1187,7 @@ int run_fused(atb_solver* s, double* const* Q, const ArkAcc& ark, cudaStream_t s
   if (grid == 0) return ATB_OK;
   {
     ProfScope ps(ATB_PROF_TEND, st);
-    s->fused(A, grid, E * op->Np, bytes(E), st);
+    s->fused(A, grid, cta_threads(E, op->Np), bytes(E), st);
   }
   const cudaError_t le = cudaGetLastError();
   if (le != cudaSuccess)
@@ -1632,7 +1637,7 @@ int atb_detail_lsrk54_steps(atb_op* op, double* const* q, double* dqbuf, double*
       A.a = rka[i];
       A.bdt = rkb[i] * dt;
       for (int k = 0; k < 5; ++k) { A.q[k] = cur[k]; A.out[k] = dq[k]; A.out2[k] = oth[k]; }
-      op->launch(A, grid, op->E * op->Np, op->smem, st);
+      op->launch(A, grid, cta_threads(op->E, op->Np), op->smem, st);
       const int rc = check_launch("tendency (no-alloc LSRK54)");
       if (rc) return rc;
       for (int k = 0; k < 5; ++k) std::swap(cur[k], oth[k]);

@@ -604,28 +604,41 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
   }
 
   // ------------------------------------------------------------ faces
-  // the face direction is dispatched to a compile-time constant so every
-  // state / normal index in the numerical flux is static (no local memory)
-  if (act) {
+  // Face-node tasks of all elements of the CTA, spread over all its threads.
+  // Each direction's 2*Nfp tasks are padded to whole warps, so a warp only
+  // ever runs faces of one direction (the flux code is not split between
+  // directions inside a warp); the direction is dispatched to a compile-time
+  // constant so every state / normal index in the numerical flux is static.
+  {
     const double lift_end = sm[2 * Nq * Nq];
-    const int ntask = 2 * DIM * Nfp + ((FUSE && LAW == LAW_EG && ((A.lin_dirs >> DZ) & 1)) ? 2 * Nfp : 0);
+    const bool lin_faces = FUSE && LAW == LAW_EG && ((A.lin_dirs >> DZ) & 1);
     const int naux_nl = FUSE ? A.naux_nl : naux;
-    for (int t = node; t < ntask; t += Np) {
+    const int fp = ((2 * Nfp + 31) / 32) * 32;
+    const int per_elem = (DIM + (lin_faces ? 1 : 0)) * fp;
+    for (int v = threadIdx.x; v < A.E * per_elem; v += blockDim.x) {
+      const int es = v / per_elem, r = v - es * per_elem;
+      const int dd = r / fp, tt = r - dd * fp;
+      const int ef = blockIdx.x * A.E + es;
+      if (tt >= 2 * Nfp || ef >= A.K) continue;
+      double* const sqe = sm + tabn + es * slotsz;
+      double* const sae = sqe + NS * Np;
+      double* const sse = sae + naux * Np + NPRE * Np;
       if constexpr (FUSE && LAW == LAW_EG) {
-        if (t >= 2 * DIM * Nfp) {
+        if (dd == DIM) {
           // z faces of the linear operator (face numbers 2*DZ, 2*DZ + 1): the
           // slot pointer is shifted so those faces land in the linear slots
-          face_task<LAW_LEG, DIM, NAuxMax<LAW_LEG, DIM>::v, DZ>(A, A.lin_law, A.lin_sflux, naux, Nq, Np, Nfp, e,
-                                                                 t - 2 * DIM * Nfp + 2 * DZ * Nfp, sq, sa,
-                                                                 ssl - (size_t)2 * DZ * Nfp * NS, gi[DZ], lift_end);
+          double* const ssle = sse + 2 * DIM * Nfp * NS + (size_t)Nfp * npl * NPVS + NS * Np;
+          face_task<LAW_LEG, DIM, NAuxMax<LAW_LEG, DIM>::v, DZ>(
+              A, A.lin_law, A.lin_sflux, naux, Nq, Np, Nfp, ef, 2 * DZ * Nfp + tt, sqe, sae,
+              ssle - (size_t)2 * DZ * Nfp * NS, __ldg(A.ginv + 3 * ef + DZ), lift_end);
           continue;
         }
       }
-      const int face = t / Nfp;
-      switch (face >> 1) {
-        case 0: face_task<LAW, DIM, NAM, 0>(A, L, A.sflux, naux_nl, Nq, Np, Nfp, e, t, sq, sa, ss, gi[0], lift_end); break;
-        case 1: if constexpr (DIM > 1) face_task<LAW, DIM, NAM, 1>(A, L, A.sflux, naux_nl, Nq, Np, Nfp, e, t, sq, sa, ss, gi[1], lift_end); break;
-        default: if constexpr (DIM > 2) face_task<LAW, DIM, NAM, 2>(A, L, A.sflux, naux_nl, Nq, Np, Nfp, e, t, sq, sa, ss, gi[2], lift_end); break;
+      const int t = 2 * dd * Nfp + tt;
+      switch (dd) {
+        case 0: face_task<LAW, DIM, NAM, 0>(A, L, A.sflux, naux_nl, Nq, Np, Nfp, ef, t, sqe, sae, sse, __ldg(A.ginv + 3 * ef), lift_end); break;
+        case 1: if constexpr (DIM > 1) face_task<LAW, DIM, NAM, 1>(A, L, A.sflux, naux_nl, Nq, Np, Nfp, ef, t, sqe, sae, sse, __ldg(A.ginv + 3 * ef + 1), lift_end); break;
+        default: if constexpr (DIM > 2) face_task<LAW, DIM, NAM, 2>(A, L, A.sflux, naux_nl, Nq, Np, Nfp, ef, t, sqe, sae, sse, __ldg(A.ginv + 3 * ef + 2), lift_end); break;
       }
     }
   }
