@@ -41,10 +41,20 @@ class DeviceOp:
         self.dg = dg
         self.ns = dg.law.numberofstates
         desc, keep = make_desc(dg)
-        aux = np.ascontiguousarray(dg.auxstate_host(), dtype=np.float64)
         h = C.c_void_p()
-        _lib.check(_lib.lib().atb_op_create(C.byref(desc), _lib.dptr(aux) if aux.size else None, C.byref(h)))
-        self.h = h
+        dev_aux = getattr(dg, "_aux_dev", None)
+        if dev_aux is not None:
+            # aux evaluated on the device: create with zeros, then copy device to device
+            _lib.check(_lib.lib().atb_op_create(C.byref(desc), None, C.byref(h)))
+            self.h = h
+            _lib.check(_lib.lib().atb_op_set_aux(h, C.cast(C.c_void_p(dev_aux.data_ptr()), _lib._DP),
+                                                 _lib.stream_ptr()))
+            import torch
+            torch.cuda.current_stream().synchronize()
+        else:
+            aux = np.ascontiguousarray(dg.auxstate_host(), dtype=np.float64)
+            _lib.check(_lib.lib().atb_op_create(C.byref(desc), _lib.dptr(aux) if aux.size else None, C.byref(h)))
+            self.h = h
         self._keep = keep
 
     def __del__(self):

@@ -50,6 +50,7 @@ SIGNATURES = {
     "atb_op_create": [C.POINTER(OpDesc), _DP, C.POINTER(C.c_void_p)],
     "atb_op_destroy": [_VP],
     "atb_op_dims": [_VP, _IP, _IP, _IP],
+    "atb_op_set_aux": [_VP, _DP, _VP],
     "atb_op_create_batch": [C.POINTER(OpDesc), C.c_int, C.POINTER(_DP), C.POINTER(C.c_void_p)],
     "atb_op_instances": [_VP, _IP, _IP],
     "atb_op_autotune": [_VP, PtrArr, _DP, _VP, _IP],

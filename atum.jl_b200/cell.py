@@ -171,6 +171,39 @@ class BrickGrid:
         return self._points
 
 
+def points_device(grid: "BrickGrid", device="cuda"):
+    """Node coordinates as a (dim, K, Np) float64 torch tensor computed on the
+    device, in the same storage order and with the same arithmetic as
+    ``grid.points()`` (for grids too large to build on the host)."""
+    import torch
+
+    c = grid.cell
+    dim, Nq, Np, K, Kd = grid.dim, c.Nq, c.Np, grid.K, grid.Kd
+    e = torch.arange(K, device=device, dtype=torch.int64)
+    idx = [None] * dim
+    if grid.stacked:
+        idx[dim - 1] = e % Kd[dim - 1]
+        r = e // Kd[dim - 1]
+        for d in range(dim - 1):
+            idx[d] = r % Kd[d]
+            r = r // Kd[d]
+    else:
+        r = e
+        for d in range(dim):
+            idx[d] = r % Kd[d]
+            r = r // Kd[d]
+    node = torch.arange(Np, device=device, dtype=torch.int64)
+    nodes = torch.as_tensor(np.asarray(c.nodes, dtype=np.float64), device=device)
+    x = torch.empty((dim, K, Np), dtype=torch.float64, device=device)
+    for d in range(dim):
+        v = torch.as_tensor(np.asarray(grid.vertices[d], dtype=np.float64), device=device)
+        v0 = v[idx[d]][:, None]
+        v1 = v[idx[d] + 1][:, None]
+        xi = nodes[(node // Nq ** d) % Nq][None, :]
+        x[d] = (v0 * (1 - xi) + v1 * (1 + xi)) / 2
+    return x
+
+
 def brickgrid(cell: LobattoCell, vertices, periodic=None, ordering: str = "cartesian") -> BrickGrid:
     """``brickgrid(cell, (vx, vy, ...); periodic, ordering)``.
 

@@ -592,7 +592,17 @@ int op_create_impl(const atb_op_desc* descs, int n, const double* const* aux_hos
 
 extern "C" int atb_op_create(const atb_op_desc* d, const double* aux_host, atb_op** out) {
   const double* aux[1] = {aux_host};
-  return op_create_impl(d, 1, aux, out);
+  // no aux values given: start from zeros, to be filled by atb_op_set_aux
+  return op_create_impl(d, 1, aux, out, d && d->naux > 0 && !aux_host);
+}
+
+extern "C" int atb_op_set_aux(atb_op* op, const double* aux, void* stream) {
+  if (!op || (!aux && op->naux > 0)) return fail(ATB_ERR_INVALID, "null argument");
+  if (op->naux == 0) return ATB_OK;
+  // host or device source: unified addressing picks the direction
+  CK(cudaMemcpyAsync(op->d_aux, aux, (size_t)op->naux * op->stride() * sizeof(double), cudaMemcpyDefault,
+                     (cudaStream_t)stream));
+  return ATB_OK;
 }
 
 extern "C" int atb_op_create_batch(const atb_op_desc* descs, int n, const double* const* aux_hosts, atb_op** out) {
@@ -967,9 +977,6 @@ int build_band(atb_solver* s, cudaStream_t st) {
   CK(cudaMemcpy(s->d_e0, e0.data(), e0.size() * sizeof(int), cudaMemcpyHostToDevice));
   M.e0 = s->d_e0;
   const int W = 2 * M.bw + 1;
-  const size_t bandn = (size_t)M.nlines * M.nunk * W;
-  if ((rc = dalloc(&s->band, bandn))) return rc;
-  CK(cudaMemsetAsync(s->band, 0, bandn * sizeof(double), st));
   double *P = nullptr, *LP = nullptr;
   const size_t fsz = (size_t)ns * M.stride;
   if ((rc = dalloc(&P, fsz))) return rc;
@@ -977,33 +984,46 @@ int build_band(atb_solver* s, cudaStream_t st) {
   double *pp[5], *lp[5];
   field_ptrs(P, ns, M.stride, pp);
   field_ptrs(LP, ns, M.stride, lp);
-  CK(cudaMemsetAsync(P, 0, fsz * sizeof(double), st));
-  for (int c = 0; c < W && rc == ATB_OK; ++c) {
-    launch_probe_fill(M, c, pp, st);
-    rc = run_tendency(L, EPI_SET, pp, lp, nullptr, 0, 0, st);
-    if (!rc) launch_band_extract(M, c, lp, s->band, st);
-  }
-  cudaFree(P);
-  cudaFree(LP);
-  if (rc) return rc;
-  // one factor per distinct column: the probed operators of a horizontally
-  // uniform problem are bitwise identical in every column -> keep one copy
+  auto probe_all = [&](auto&& extract) -> int {
+    CK(cudaMemsetAsync(P, 0, fsz * sizeof(double), st));
+    int r = ATB_OK;
+    for (int c = 0; c < W && r == ATB_OK; ++c) {
+      launch_probe_fill(M, c, pp, st);
+      r = run_tendency(L, EPI_SET, pp, lp, nullptr, 0, 0, st);
+      if (!r) extract(c);
+    }
+    return r;
+  };
+  // pass 1: line 0's band, and whether every column's probed operator is
+  // bitwise the same (horizontally uniform problems) -> one shared factor
+  double* one = nullptr;
   int* d_nd = nullptr;
-  if ((rc = dalloc(&d_nd, 1))) return rc;
+  const size_t rs = 2 * (size_t)(M.bw + 1);
+  double* band1 = nullptr;
+  if ((rc = dalloc(&band1, (size_t)M.nunk * W)) || (rc = dalloc(&d_nd, 1))) {
+    cudaFree(P); cudaFree(LP); cudaFree(band1);
+    return rc;
+  }
+  CK(cudaMemsetAsync(band1, 0, (size_t)M.nunk * W * sizeof(double), st));
   CK(cudaMemsetAsync(d_nd, 0, sizeof(int), st));
-  launch_band_compare(M, s->band, d_nd, st);
-  int nd = 0;
-  CK(cudaMemcpyAsync(&nd, d_nd, sizeof(int), cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
+  rc = probe_all([&](int c) { launch_band_extract_first(M, c, lp, band1, d_nd, st); });
+  int nd = 1;
+  if (!rc) {
+    CK(cudaMemcpyAsync(&nd, d_nd, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+  }
   cudaFree(d_nd);
   const double scale = -s->dt * s->ima[2][2];  // M = I - dt a_ii L (src/odesolvers.jl:264-268)
-  if (nd == 0) {
-    double* one = nullptr;
-    if ((rc = dalloc(&one, (size_t)M.nunk * 2 * (M.bw + 1)))) return rc;
-    launch_band_compact(M, s->band, one, st);
-    launch_band_factor(M.nunk, M.bw, 1, one, 2 * (M.bw + 1), 1, scale, st);
+  if (!rc && nd == 0) {
+    cudaFree(P);
+    cudaFree(LP);
+    if ((rc = dalloc(&one, (size_t)M.nunk * rs))) { cudaFree(band1); return rc; }
+    LineMap M1 = M;
+    M1.nlines = 1;  // band1 holds one line
+    launch_band_compact(M1, band1, one, st);
+    launch_band_factor(M.nunk, M.bw, 1, one, (int)rs, 1, scale, st);
     CK(cudaStreamSynchronize(st));
-    cudaFree(s->band);
+    cudaFree(band1);
     s->band = one;
     s->ld = 1;
     // per-element inverses for the block-parallel solve
@@ -1011,9 +1031,23 @@ int build_band(atb_solver* s, cudaStream_t st) {
     if ((rc = dalloc(&s->blk, (size_t)M.KV * 4 * BW1 * BW1))) return rc;
     launch_block_prep(s->band, M.KV, BW1, s->blk, st);
     CK(cudaStreamSynchronize(st));
-  } else {
+  } else if (!rc) {
+    // pass 2: columns differ -> one band and one factor per line
+    cudaFree(band1);
+    const size_t bandn = (size_t)M.nlines * M.nunk * W;
+    if ((rc = dalloc(&s->band, bandn))) { cudaFree(P); cudaFree(LP); return rc; }
+    CK(cudaMemsetAsync(s->band, 0, bandn * sizeof(double), st));
+    rc = probe_all([&](int c) { launch_band_extract(M, c, lp, s->band, st); });
+    cudaFree(P);
+    cudaFree(LP);
+    if (rc) return rc;
     launch_band_factor(M.nunk, M.bw, M.nlines, s->band, W, M.nlines, scale, st);
     s->ld = M.nlines;
+  } else {
+    cudaFree(P);
+    cudaFree(LP);
+    cudaFree(band1);
+    return rc;
   }
   if ((rc = check_launch("band factor"))) return rc;
   return ATB_OK;
@@ -1426,7 +1460,10 @@ extern "C" int atb_solver_create(int kind, atb_op* rhs, atb_op* linrhs, double d
     std::memcpy(s->imb, exb, sizeof(exb));
     std::memcpy(s->exc, exc, sizeof(exc));
     std::memcpy(s->imc, exc, sizeof(exc));
-    if ((rc = dalloc(&s->Qs, 2 * fsz)) || (rc = dalloc(&s->exK, 3 * fsz)) || (rc = dalloc(&s->imK, 3 * fsz))) {
+    // the accumulated stages (rhs and linrhs, split_rhs = false) keep one
+    // explicit-tendency buffer; the general path keeps all three stages'
+    const size_t nex = (rhs && linrhs && !split_rhs) ? 1 : 3;
+    if ((rc = dalloc(&s->Qs, 2 * fsz)) || (rc = dalloc(&s->exK, nex * fsz)) || (rc = dalloc(&s->imK, 3 * fsz))) {
       solver_free(s);
       return rc;
     }

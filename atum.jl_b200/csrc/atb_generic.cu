@@ -110,6 +110,42 @@ void launch_band_extract(const LineMap& M, int color, const double* const* LP, d
   band_extract_kernel<<<grid_for(total, 256), 256, 0, st>>>(M, color, p[0], p[1], p[2], p[3], p[4], band);
 }
 
+// Line 0's probed columns into a single band (layout of band_extract with one
+// line), and a count of the lines whose probed values differ bitwise from
+// line 0's: with none, every column shares one factor and no per-line band
+// is ever stored.
+__global__ void band_extract_first_kernel(const LineMap M, int color, const double* L0, const double* L1,
+                                          const double* L2, const double* L3, const double* L4, double* band1,
+                                          int* ndiff) {
+  const double* LP[5] = {L0, L1, L2, L3, L4};
+  const int W = 2 * M.bw + 1;
+  const size_t total = (size_t)M.nlines * M.nunk;
+  int local = 0;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int line = (int)(t % M.nlines);
+    const int r = (int)(t / M.nlines);
+    int delta = ((color - r) % W + W) % W;
+    int j = delta <= M.bw ? r + delta : r + delta - W;
+    if (j < 0 || j >= M.nunk) continue;
+    const int s = r % M.ns, kvg = r / M.ns;
+    const int ev = kvg / M.Nq, kv = kvg - ev * M.Nq;
+    const double v = LP[s][line_gid(M, line, ev, kv)];
+    const double v0 = LP[s][line_gid(M, 0, ev, kv)];
+    if (line == 0) band1[(size_t)r * W + (j - r + M.bw)] = v;
+    if (__double_as_longlong(v) != __double_as_longlong(v0)) local = 1;
+  }
+  if (local) atomicAdd(ndiff, 1);
+}
+
+void launch_band_extract_first(const LineMap& M, int color, const double* const* LP, double* band1, int* ndiff,
+                               cudaStream_t st) {
+  size_t total = (size_t)M.nlines * M.nunk;
+  const double* p[5] = {LP[0], LP[0], LP[0], LP[0], LP[0]};
+  for (int s = 0; s < M.ns; ++s) p[s] = LP[s];
+  band_extract_first_kernel<<<grid_for(total, 256), 256, 0, st>>>(M, color, p[0], p[1], p[2], p[3], p[4], band1,
+                                                                  ndiff);
+}
+
 // M = I + scale * A, then LU without pivoting, in place (one thread per
 // matrix).  Entry (i, j) lives at band[(i * rs + (j - i + bw)) * ld + l].
 __global__ void band_factor_kernel(int n, int bw, int nl, double* band, int rs, int ld, double scale) {

@@ -48,6 +48,9 @@ struct LineMap {
 void launch_probe_fill(const LineMap& M, int color, double* const* P, cudaStream_t st);
 // probed band layout (one matrix per line): band[(r * W + (j - r + bw)) * nlines + line]
 void launch_band_extract(const LineMap& M, int color, const double* const* LP, double* band, cudaStream_t st);
+// line 0's band (one line) plus a count of lines differing from it bitwise
+void launch_band_extract_first(const LineMap& M, int color, const double* const* LP, double* band1, int* ndiff,
+                               cudaStream_t st);
 void launch_band_compare(const LineMap& M, const double* band, int* ndiff, cudaStream_t st);
 // copy line 0 into a compact matrix with padded row stride rs = 2*(bw+1)
 void launch_band_compact(const LineMap& M, const double* band, double* out, cudaStream_t st);

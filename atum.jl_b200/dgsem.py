@@ -50,12 +50,28 @@ class DGSEM:
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
         self.precision = precision
-        self._aux = None if auxstate is None else self._as_aux(auxstate)
+        self._aux_dev = None
+        if auxstate is not None and getattr(auxstate, "is_cuda", False):
+            # aux evaluated on the device (like the reference's
+            # auxiliary.(law, points(grid)) on GPU arrays): kept there, uploaded
+            # device to device, copied to the host only if a host copy is asked for
+            import torch
+
+            want = (self.law.naux, len(self.grid), self.grid.cell.Np)
+            if auxstate.numel() != int(np.prod(want)):
+                raise ValueError(f"auxstate must have shape {want}")
+            self._aux_dev = auxstate.detach().to(dtype=torch.float64).reshape(want).contiguous()
+            self._aux = None
+        else:
+            self._aux = None if auxstate is None else self._as_aux(auxstate)
         self._dev = None
 
     # ------------------------------------------------------------- host spec
     def _as_aux(self, auxstate):
         if isinstance(auxstate, DGSEM):
+            if auxstate._aux_dev is not None and auxstate._aux is None:
+                self._aux_dev = auxstate._aux_dev
+                return None
             auxstate = auxstate.auxstate_host()
         if hasattr(auxstate, "detach"):
             auxstate = auxstate.detach().cpu().numpy()
@@ -67,7 +83,10 @@ class DGSEM:
 
     def auxstate_host(self) -> np.ndarray:
         if self._aux is None:
-            self._aux = np.ascontiguousarray(self.law.auxiliary(self.grid.points()), dtype=np.float64)
+            if self._aux_dev is not None:
+                self._aux = self._aux_dev.cpu().numpy()
+            else:
+                self._aux = np.ascontiguousarray(self.law.auxiliary(self.grid.points()), dtype=np.float64)
         return self._aux
 
     @property

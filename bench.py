@@ -475,7 +475,191 @@ def run_serve(args):
     return 0
 
 
-# ------------------------------------------- batched shallow-water instances
+# ---------------------------------------------------- large single instance
+def run_c5(args):
+    """3-D Euler-gravity on 128 x 128 x 32 hexahedra, N = 7 (1.342 G DOFs) in
+    a 40 km x 40 km x 10 km box (isotropic 312.5 m elements), periodic
+    laterally, reflective walls top and bottom; constant-theta hydrostatic
+    background (theta0 = 300 K) with a seeded smooth theta perturbation of
+    +-0.5 K (random Fourier modes of wavelengths 4-16 elements); IMEX ARK23
+    (split_rhs = false, vertical acoustics through the banded column solve).
+    Grid points, aux fields and the initial state are built on the device.
+    The same 50 steps run with FP64 flux arithmetic and with the FP32-flux
+    form; reported: both throughputs, the FP32-flux error against FP64, mass
+    drift, and per-kernel times with roofline fractions."""
+    import numpy as np
+    import torch
+
+    dist, rank, world = dist_init()
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    A = load_pkg()
+    from atum_b200 import _lib
+    from atum_b200.cell import points_device
+    import problems as P
+
+    Kx, Ky, Kz = args.c5_elements
+    N = 7
+    steps = args.steps if args.steps is not None else 50
+    Lh, H = 40e3 * Kx / 128, 10e3 * Kz / 32
+    vx = np.array([Lh * i / Kx for i in range(Kx + 1)])
+    vy = np.array([Lh * i / Ky for i in range(Ky + 1)])
+    vz = np.array([H * i / Kz for i in range(Kz + 1)])
+    cell = A.LobattoCell(N + 1, N + 1, N + 1)
+    grid = A.brickgrid(cell, (vx, vy, vz), periodic=(True, True, False), ordering="stacked")
+    law = A.EulerGravityLaw(3, grav=9.81, problem=A.ReflectiveWall(referencestate=P._bubble_reference))
+    g = law.grav
+    cv = 719.0
+    cp = law.gamma * cv
+    R = cp - cv
+    x = points_device(grid)
+    z = x[2]
+    pi_ex = 1 - g / (cp * 300.0) * z
+    aux = torch.zeros((law.naux,) + tuple(z.shape), dtype=torch.float64, device="cuda")
+    aux[0] = g * z
+    aux[3] = g
+    aux[4] = 1e5 / (R * 300.0) * pi_ex ** (cv / R)
+    aux[5] = 1e5 * pi_ex ** (cp / R)
+    # smooth seeded theta perturbation: random modes, wavelengths 4-16 elements
+    rng = np.random.default_rng(20261203)
+    dth = torch.zeros_like(z)
+    he = Lh / Kx
+    for _ in range(24):
+        lam = rng.uniform(4, 16, 3) * he
+        kx = 2 * np.pi * max(1, round(Lh / lam[0])) / Lh * rng.choice([-1, 1])
+        ky = 2 * np.pi * max(1, round(Lh / lam[1])) / Lh * rng.choice([-1, 1])
+        kz = 2 * np.pi / lam[2]
+        dth += rng.standard_normal() * torch.cos(kx * x[0] + ky * x[1] + kz * z + rng.uniform(0, 2 * np.pi))
+    dth *= 0.5 / dth.abs().max()
+    del x
+    p = aux[5]
+    rho = p / (R * (300.0 + dth) * pi_ex)
+    del dth, pi_ex
+    q0 = torch.zeros((5,) + tuple(z.shape), dtype=torch.float64, device="cuda")
+    q0[0] = rho
+    q0[4] = p / (law.gamma - 1) + rho * aux[0]
+    del rho, p, z
+    dofs = q0.numel()
+    lin = A.LinearEulerGravityLaw(law)
+    lindg = A.DGSEM(law=lin, grid=grid, surface_numericalflux=A.RusanovFlux(), auxstate=aux, directions=(3,))
+    dz = A.min_node_distance(grid, dims=(3,))
+    dt = 0.25 * dz / 340.0
+    w = torch.as_tensor(np.asarray(cell.weights, dtype=np.float64), device="cuda")
+    w3 = (w[:, None, None] * w[None, :, None] * w[None, None, :]).reshape(-1)  # node order i fastest
+    L = _lib.lib()
+    peak_fp64 = _lib.C.c_double()
+    _lib.check(L.atb_probe_fp64_peak(_lib.C.byref(peak_fp64), _lib.stream_ptr()))
+    peaks, kind = measured_peaks()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def run(precision):
+        dg = A.DGSEM(law=law, grid=grid, volume_form=A.FluxDifferencingForm(A.EntropyConservativeFlux()),
+                     surface_numericalflux=A.RusanovFlux(), auxstate=aux, precision=precision)
+        torch.cuda.empty_cache()
+        q = q0.clone()
+        s = A.ARK23(dg, lindg, q, dt, split_rhs=False)
+        s.step(q, args.warmup)
+        q.copy_(q0)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n0 = _lib.C.c_long()
+        L.atb_launch_count(_lib.C.byref(n0))
+        e0.record()
+        s.step(q, steps)
+        e1.record()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        n1 = _lib.C.c_long()
+        L.atb_launch_count(_lib.C.byref(n1))
+        # per-kernel times: a few more steps with the library's launch events
+        qp = q.clone()
+        _lib.check(L.atb_profile_reset())
+        _lib.check(L.atb_profile_enable(1))
+        s.step(qp, 3)
+        barrier()
+        _lib.check(L.atb_profile_enable(0))
+        prof = {}
+        for k, name in enumerate(("tendency", "tendency_linear", "band_solve", "combine", "reduce")):
+            nl, tm = _lib.C.c_long(), _lib.C.c_double()
+            _lib.check(L.atb_profile_read(k, _lib.C.byref(nl), _lib.C.byref(tm)))
+            prof[name] = {"launches": nl.value, "ms": tm.value}
+        del qp, s, dg
+        import gc
+        gc.collect()  # the operator and its spec refer to each other
+        torch.cuda.empty_cache()
+        return q, ms, int(n1.value - n0.value), prof
+
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        q64, ms64, nl64, prof64 = run("fp64")
+        q32, ms32, nl32, prof32 = run("fp32flux")
+    assert torch.isfinite(q64).all() and torch.isfinite(q32).all(), "non-finite state"
+
+    def wnorm2(a):
+        return float(sum(((a[c] ** 2) * w3[None, :]).sum() for c in range(a.shape[0])))
+
+    rel = math.sqrt(wnorm2(q32 - q64) / wnorm2(q64))
+    pert = math.sqrt(wnorm2(q32 - q64) / wnorm2(q64 - q0))
+    m0 = float((q0[0] * w3[None, :]).sum())
+    drift64 = abs(float((q64[0] * w3[None, :]).sum()) - m0) / m0
+    drift32 = abs(float((q32[0] * w3[None, :]).sum()) - m0) / m0
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+
+    def kernels(prof, precision):
+        out = {}
+        fused = prof["tendency_linear"]["launches"] == 0
+        t = prof["tendency"]
+        avg = t["ms"] / max(1, t["launches"])
+        fl = (FLOPS_PER_DOF_STAGE["bubble_3d_N7_ec_rusanov"] +
+              (FLOPS_PER_DOF_STAGE["bubble_3d_N7_linear_weak_z"] if fused else 0.0)) * dofs
+        out["stage_kernel"] = {"kernel": "tendency_kernel<EulerGravity,3,%s,Nq=8%s>" %
+                               ("EC" if precision == "fp64" else "EC32", ",fused" if fused else ""),
+                               "avg_launch_ms": avg, "bound": "fp64", "achieved_tflops": fl / (avg * 1e-3) / 1e12,
+                               "peak_tflops": peak_fp64.value,
+                               "frac": fl / (avg * 1e-3) / 1e12 / peak_fp64.value}
+        b = prof["band_solve"]
+        if b["launches"]:
+            avgb = b["ms"] / b["launches"]
+            # right-hand side read, solution written, read back and rewritten
+            byt = 4 * dofs * 8
+            out["band_solve"] = {"kernel": "band_solve_mma_kernel<8,5>", "avg_launch_ms": avgb, "bound": "hbm",
+                                 "achieved_gbs": byt / (avgb * 1e-3) / 1e9, "peak_gbs": peaks["hbm_gbs"],
+                                 "frac": byt / (avgb * 1e-3) / 1e9 / peaks["hbm_gbs"], "peak_kind": kind}
+        out["launch_totals"] = prof
+        return out
+
+    v64 = world * dofs * 3 * steps / (ms64 * 1e-3)
+    v32 = world * dofs * 3 * steps / (ms32 * 1e-3)
+    line = {
+        "metric": "DOF-stage updates/s", "value": v64, "unit": "DOF-stage/s", "n_gpus": world, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": ms64 / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (built on the device)",
+        "config": {"workload": f"3-D Euler-gravity, {Kx}x{Ky}x{Kz} hexahedra, N=7 ({dofs} DOFs), hydrostatic "
+                               "background + seeded smooth theta' (+-0.5 K), EC volume + Rusanov surface flux, "
+                               "IMEX ARK23 split_rhs=false, vertical banded solve",
+                   "dofs": dofs, "stages_per_step": 3, "box_m": [Lh, Lh, H], "dt_s": dt,
+                   "l2": f"working set ~{dofs * 8 * 12 / 1e9:.0f} GB >> 126 MB L2 (no flush)"},
+        "gpu_launches": nl64,
+        "fp32flux": {"value": v32, "ms_per_step": ms32 / steps, "gpu_launches": nl32,
+                     "speedup_vs_fp64": v32 / v64,
+                     "rel_l2_vs_fp64": rel, "rel_l2_vs_fp64_of_perturbation": pert},
+        "mass_drift": {"fp64": drift64, "fp32flux": drift32},
+        "kernels": {"fp64": kernels(prof64, "fp64"), "fp32flux": kernels(prof32, "fp32flux")},
+        "clocks": clk.summary(),
+        "e2e": None,
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+# ------------------------------------------- batched shallow-water instances# ------------------------------------------- batched shallow-water instances
 def run_swbatch(args):
     """256 rotating shallow-water instances (f-plane, g = 9.81), each a
     periodic 32 x 32 square of N = 4 elements with its own seeded bathymetry
@@ -627,9 +811,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32flux"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="bubble", choices=["bubble", "swbatch", "serve"],
+    ap.add_argument("--workload", default="bubble", choices=["bubble", "swbatch", "serve", "c5"],
                     help="bubble: 3-D rising bubble, IMEX ARK23 (default); swbatch: packed shallow-water "
-                         "instances; serve: Poisson request stream through the serving loop")
+                         "instances; serve: Poisson request stream through the serving loop; c5: 128x128x32 "
+                         "hexahedra at N=7, FP64 and FP32-flux")
+    ap.add_argument("--c5-elements", type=int, nargs=3, default=[128, 128, 32],
+                    help="element counts of the c5 workload (smaller counts for a quick run)")
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--requests", type=int, default=2000)
     ap.add_argument("--rate", type=float, default=200.0)
@@ -644,6 +831,8 @@ def main():
         return run_swbatch(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "c5":
+        return run_c5(args)
     if args.steps is None:
         args.steps = 100
     if args.impl == "reference":

@@ -102,8 +102,15 @@ const char* atb_last_error(void);
 int atb_device_count(int* n);
 
 /* DGSEM construction (src/dgsem.jl:38-56); aux_host: naux*K*Np values in the
- * field layout, evaluated on the host like auxiliary.(law, points(grid)). */
+ * field layout, evaluated on the host like auxiliary.(law, points(grid)).
+ * aux_host may be NULL: the aux fields then start at zero and are meant to be
+ * filled by atb_op_set_aux. */
 int atb_op_create(const atb_op_desc* desc, const double* aux_host, atb_op** out);
+/* Replaces the aux fields (naux*K*Np values, component-major) from host or
+ * device memory -- the reference evaluates auxiliary.(law, points(grid)) on
+ * the device (src/dgsem.jl:47-49); a caller that does the same passes its
+ * device array here.  Ordered on `stream`. */
+int atb_op_set_aux(atb_op* op, const double* aux, void* stream);
 int atb_op_destroy(atb_op* op);
 int atb_op_dims(const atb_op* op, int* ns, int* K, int* Np);
 
