@@ -428,15 +428,16 @@ int op_create_impl(const atb_op_desc* descs, int n, const double* const* aux_hos
     switch (d->volume_flux) {
       case ATB_FLUX_CENTRAL: vk = VK_CENTRAL; break;
       case ATB_FLUX_EC: vk = (d->precision == ATB_PREC_FP32FLUX) ? VK_EC32 : VK_EC; break;
-      case ATB_FLUX_KG: vk = VK_KG; break;
+      case ATB_FLUX_KG: vk = (d->precision == ATB_PREC_FP32FLUX) ? VK_KG32 : VK_KG; break;
       default: return fail(ATB_ERR_INVALID, "no two-point volume flux %d", d->volume_flux);
     }
   }
   if (d->precision == ATB_PREC_FP32FLUX &&
-      !(vk == VK_EC32 && (d->law == LAW_EULER || d->law == LAW_EG || d->law == LAW_SW)))
+      !((vk == VK_EC32 && (d->law == LAW_EULER || d->law == LAW_EG || d->law == LAW_SW)) ||
+        (vk == VK_KG32 && (d->law == LAW_EULER || d->law == LAW_EG))))
     return fail(ATB_ERR_INVALID,
-                "the FP32-flux form exists for the entropy-conservative flux-differencing volume term of "
-                "Euler, Euler-gravity and shallow water");
+                "the FP32-flux form exists for the flux-differencing volume term with the entropy-conservative "
+                "flux (Euler, Euler-gravity, shallow water) or the Kennedy-Gruber flux (Euler, Euler-gravity)");
   tend_launch_fn fn = nullptr;
   red_launch_fn rf = nullptr;
   // a compile-time node-count specialisation when one exists, else the

@@ -19,6 +19,9 @@ template <> tend_launch_fn pick_launcher<LAW_EG>(int dim, int vk) {
   if (dim == 1 && vk == VK_EC32) return tend_launch<LAW_EG, 1, VK_EC32, 0>;
   if (dim == 2 && vk == VK_EC32) return tend_launch<LAW_EG, 2, VK_EC32, 0>;
   if (dim == 3 && vk == VK_EC32) return tend_launch<LAW_EG, 3, VK_EC32, 0>;
+  if (dim == 1 && vk == VK_KG32) return tend_launch<LAW_EG, 1, VK_KG32, 0>;
+  if (dim == 2 && vk == VK_KG32) return tend_launch<LAW_EG, 2, VK_KG32, 0>;
+  if (dim == 3 && vk == VK_KG32) return tend_launch<LAW_EG, 3, VK_KG32, 0>;
   return nullptr;
 }
 template <> red_launch_fn pick_reducer<LAW_EG>(int dim) {

@@ -7,6 +7,7 @@ tend_launch_fn pick_nq_sw_2_vk_ec32(int nq);
 tend_launch_fn pick_nq_eg_3_vk_ec32(int nq);
 tend_launch_fn pick_nq_eg_3_vk_ec(int nq);
 tend_launch_fn pick_nq_eg_3_vk_kg(int nq);
+tend_launch_fn pick_nq_eg_3_vk_kg32(int nq);
 tend_launch_fn pick_nq_eg_3_vk_weak(int nq);
 tend_launch_fn pick_nq_eg_2_vk_ec(int nq);
 tend_launch_fn pick_nq_leg_3_vk_weak(int nq);
@@ -30,6 +31,7 @@ template <> tend_launch_fn pick_launcher_nq<LAW_EG>(int dim, int vk, int nq) {
   if (dim == 3 && vk == VK_EC32) return pick_nq_eg_3_vk_ec32(nq);
   if (dim == 3 && vk == VK_EC) return pick_nq_eg_3_vk_ec(nq);
   if (dim == 3 && vk == VK_KG) return pick_nq_eg_3_vk_kg(nq);
+  if (dim == 3 && vk == VK_KG32) return pick_nq_eg_3_vk_kg32(nq);
   if (dim == 3 && vk == VK_WEAK) return pick_nq_eg_3_vk_weak(nq);
   if (dim == 2 && vk == VK_EC) return pick_nq_eg_2_vk_ec(nq);
   (void)dim; (void)vk; (void)nq;

@@ -46,7 +46,9 @@ namespace atb {
 
 // VK_EC32: the entropy-conservative volume flux in the FP32-flux precision
 // form (mixed: balance-critical terms in FP64 adds/multiplies, the rest FP32)
-enum { VK_WEAK = 0, VK_CENTRAL = 1, VK_EC = 2, VK_KG = 3, VK_EC32 = 4 };
+// VK_KG32: the Kennedy-Gruber volume flux in the FP32-flux precision form
+// (FP64 rho and p averages, FP32 velocities, energies and products)
+enum { VK_WEAK = 0, VK_CENTRAL = 1, VK_EC = 2, VK_KG = 3, VK_EC32 = 4, VK_KG32 = 5 };
 enum { EPI_SET = 0, EPI_ADD = 1, EPI_LSRK = 2, EPI_SUBOUT2 = 3, EPI_RLSRK = 4, EPI_ARK = 5 };
 
 // neighbour-table encoding: relative offsets for interior faces, so an
@@ -92,6 +94,7 @@ template <int LAW, int DIM, int VK> struct NPre {
   static constexpr int v = (VK == VK_EC)     ? ((LAW == LAW_SW) ? DIM + 1 : DIM + 3)
                            : (VK == VK_KG)   ? DIM + 2
                            : (VK == VK_EC32) ? ((LAW == LAW_SW) ? (DIM + 2) / 2 : 3 + (DIM + 2) / 2)
+                           : (VK == VK_KG32) ? 1 + (DIM + 2) / 2
                                              : DIM * NS;
 };
 // upper bound of the aux components a kernel stages (compile time, so the
@@ -267,6 +270,24 @@ __device__ __forceinline__ void kg_vol(int d, T r1, const T* P1, T r2, const T* 
   f[DIM + 1] = ud * (rho_avg * e_avg + p_avg);
 }
 
+// Kennedy-Gruber flux, row d, FP32-flux precision form: the density and
+// pressure averages -- the pressure term balances the FP64 gravity fluctuation
+// of a hydrostatic state -- stay FP64; velocities, the specific energy and the
+// advective products are FP32.
+template <int DIM>
+__device__ __forceinline__ void kg_vol32(int d, double r1, double p1, const float* u1, float e1, double r2, double p2,
+                                         const float* u2, float e2, double* f) {
+  const double rho_avg = (r1 + r2) * 0.5, p_avg = (p1 + p2) * 0.5;
+  const float rf = (float)rho_avg;
+  const float ud = 0.5f * (u1[d] + u2[d]);
+  f[0] = (double)(ud * rf);
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) f[1 + c] = (double)(ud * ((0.5f * (u1[c] + u2[c])) * rf));
+  f[1 + d] = f[1 + d] + p_avg;
+  const float e_avg = 0.5f * (e1 + e2);
+  f[DIM + 1] = (double)(ud * (rf * e_avg)) + (double)ud * p_avg;
+}
+
 // pair index of nodes a < b on a line of Nq nodes
 __device__ __forceinline__ int pair_index(int a, int b, int Nq) { return a * Nq - a * (a + 1) / 2 + (b - a - 1); }
 
@@ -330,7 +351,7 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
   constexpr int NS = NSt<LAW, DIM>::v;
   constexpr int NPRE = NPre<LAW, DIM, VK>::v;
   constexpr int NAM = NAuxMax<LAW, DIM>::v;
-  constexpr bool PAIRS = (VK == VK_EC || VK == VK_KG || VK == VK_EC32);
+  constexpr bool PAIRS = (VK == VK_EC || VK == VK_KG || VK == VK_EC32 || VK == VK_KG32);
   constexpr int PR_IDX = (VK == VK_EC32) ? 2 : DIM + 2;  // p/rho in the own-node values
   constexpr int NPV = PAIRS ? NPairVals<LAW, DIM, VK>::v : 0;
   constexpr int NPVS = PAIRS ? NPairVals<LAW, DIM, VK>::stride : 0;
@@ -402,6 +423,14 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
       for (int c = 0; c < DIM; ++c) Pn[c] = qn[1 + c] / rho;
       Pn[DIM] = pressure_eg<DIM>(L.gamma, qn, (LAW == LAW_EG) ? an[0] : 0.0);
       Pn[DIM + 1] = qn[DIM + 1] / rho;
+    } else if constexpr (VK == VK_KG32) {
+      const double rho = qn[0], rinv = 1.0 / rho;
+      Pn[0] = pressure_eg<DIM>(L.gamma, qn, (LAW == LAW_EG) ? an[0] : 0.0);
+      float* spf = (float*)(sp + Np);
+      const float rinvf = (float)rinv;
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) spf[c * Np + node] = (float)qn[1 + c] * rinvf;
+      spf[DIM * Np + node] = (float)qn[DIM + 1] * rinvf;
     } else if constexpr (VK == VK_EC32 && LAW == LAW_SW) {
       float* spf = (float*)sp;
       const float hinv = 1.f / (float)qn[0];
@@ -428,7 +457,9 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
       }
       spf[DIM * Np + node] = uu;
     }
-    if constexpr (VK == VK_EC32 && LAW != LAW_SW) {
+    if constexpr (VK == VK_KG32) {
+      sp[node] = Pn[0];
+    } else if constexpr (VK == VK_EC32 && LAW != LAW_SW) {
 #pragma unroll
       for (int k = 0; k < 3; ++k) sp[k * Np + node] = Pn[k];
     } else if constexpr (VK == VK_EC32) {
@@ -484,6 +515,17 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
           const int ab = spair[p];
           const int na = lb + (ab & 0xff) * sd, nb = lb + (ab >> 8) * sd;
           double f[NS + 1];
+          if constexpr (VK == VK_KG32) {
+            const float* spf = (const float*)(sp + Np);
+            float u1[DIM], u2[DIM];
+#pragma unroll
+            for (int c = 0; c < DIM; ++c) { u1[c] = spf[c * Np + na]; u2[c] = spf[c * Np + nb]; }
+            kg_vol32<DIM>(d, sq[na], sp[na], u1, spf[DIM * Np + na], sq[nb], sp[nb], u2, spf[DIM * Np + nb], f);
+            double* dst = spv + (size_t)t * NPVS;
+#pragma unroll
+            for (int s = 0; s < NPV; ++s) dst[s] = f[s];
+            continue;
+          }
           if constexpr (VK == VK_EC32) {
             if constexpr (LAW == LAW_SW) {
               const float* spf = (const float*)sp;
@@ -745,13 +787,14 @@ template <int LAW> tend_launch_fn pick_launcher_nq(int dim, int vk, int nq);
 inline int npre_of(int law, int dim, int vk) {
   int ns = (law == LAW_ADV) ? 1 : dim + 2;
   if (vk == VK_EC32) return (law == LAW_SW) ? (dim + 2) / 2 : 3 + (dim + 2) / 2;
+  if (vk == VK_KG32) return 1 + (dim + 2) / 2;
   if (vk == VK_EC) return (law == LAW_SW) ? dim + 1 : dim + 3;
   if (vk == VK_KG) return dim + 2;
   return dim * ns;
 }
 inline int npv_stride_of(int law, int dim, int vk) {
   int ns = (law == LAW_ADV) ? 1 : dim + 2;
-  if (vk == VK_EC || vk == VK_KG || vk == VK_EC32)
+  if (vk == VK_EC || vk == VK_KG || vk == VK_EC32 || vk == VK_KG32)
     return (ns + ((law == LAW_EG && (vk == VK_EC || vk == VK_EC32)) ? 1 : 0)) | 1;
   return 0;
 }

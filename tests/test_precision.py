@@ -50,6 +50,27 @@ def test_vortex_fp32flux():
     assert _rel(c64.dg, q32, q64) <= 1e-6
 
 
+def test_vortex_kg_fp32flux():
+    """Kennedy-Gruber volume flux in the FP32-flux form (Euler)."""
+    c64 = P.vortex_c1(vflux="kg")
+    c32 = P.vortex_c1(vflux="kg", precision="fp32flux")
+    q64, q32 = PT.to_dev(c64.q0), PT.to_dev(c32.q0)
+    A.LSRK54(c64.dg, q64, c64.dt).step(q64, 100)
+    A.LSRK54(c32.dg, q32, c32.dt).step(q32, 100)
+    assert _rel(c64.dg, q32, q64) <= 1e-6
+
+
+def test_bubble_imex_kg_fp32flux():
+    """Kennedy-Gruber FP32-flux form on the rising bubble (Euler-gravity,
+    IMEX): the FP64 pressure average keeps the hydrostatic balance."""
+    c64 = P.bubble_3d(N=4, K=6, imex=True, steps=40, vflux="kg")
+    c32 = P.bubble_3d(N=4, K=6, imex=True, steps=40, vflux="kg", precision="fp32flux")
+    q64, q32 = PT.to_dev(c64.q0), PT.to_dev(c32.q0)
+    A.ARK23(c64.dg, c64.lindg, q64, c64.dt, split_rhs=False).step(q64, 40)
+    A.ARK23(c32.dg, c32.lindg, q32, c32.dt, split_rhs=False).step(q32, 40)
+    assert _rel(c64.dg, q32, q64) <= 1e-6
+
+
 def test_shallow_water_fp32flux_and_mass():
     import torch
     c64 = P.sw_fplane(K=8, steps=50)
