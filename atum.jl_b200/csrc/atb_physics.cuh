@@ -390,6 +390,73 @@ __device__ __forceinline__ T flux_ws_recip(const LawP& L, int d, const T* q, con
   }
 }
 
+// FP32-flux precision form of flux_ws_recip: the mass flux (a state value)
+// and the pressure term stay FP64 -- the pressure difference across a face
+// balances gravity / bathymetry in a resting state -- while the reciprocal
+// of rho, the velocities, kinetic energy, advective products, the energy
+// flux product and the wave speed are FP32.
+template <int LAW, int DIM>
+__device__ __forceinline__ double flux_ws_recip32(const LawP& L, int d, const double* q, const double* aux,
+                                                  double* f) {
+  const float rinv = 1.f / (float)q[0];
+  float u[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) u[c] = (float)q[1 + c] * rinv;
+  f[0] = q[1 + d];
+  if constexpr (LAW == LAW_SW) {
+    const double p = L.grav * (q[0] * q[0]) / 2.0;
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) f[1 + c] = (double)((float)q[1 + d] * u[c]);
+    f[1 + d] = f[1 + d] + p;
+    f[DIM + 1] = (double)(u[d] * (float)q[DIM + 1]);
+    return (double)(fabsf(u[d]) + sqrtf((float)L.grav * (float)q[0]));
+  } else {
+    const double Phi = (LAW == LAW_EG) ? aux[0] : 0.0;
+    float ke = 0.f;
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) ke += (float)q[1 + c] * u[c];
+    const double p = (L.gamma - 1.0) * (q[DIM + 1] - (double)(0.5f * ke) - q[0] * Phi);
+    double dp = p;
+    if (LAW == LAW_EG && L.pde) dp = dp - aux[DIM + 2];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) f[1 + c] = (double)((float)q[1 + d] * u[c]);
+    f[1 + d] = f[1 + d] + dp;
+    f[DIM + 1] = (double)(u[d] * (float)(q[DIM + 1] + p));
+    return (double)(fabsf(u[d]) + sqrtf((float)L.gamma * (float)p * rinv));
+  }
+}
+
+// Central / Rusanov surface flux in the FP32-flux form: the two sides' fluxes
+// from flux_ws_recip32, averaged in FP64; the dissipation is the FP64 jump
+// times an FP32 wave speed.  Other surface fluxes keep their FP64 form.
+template <int LAW, int DIM>
+__device__ __forceinline__ bool surface_flux32(const LawP& L, int kind, int d, double sgn, const double* qm,
+                                               const double* am, const double* qp, const double* ap, double* nf) {
+  constexpr int NS = NSt<LAW, DIM>::v;
+  if constexpr (LAW == LAW_EULER || LAW == LAW_EG || LAW == LAW_SW) {
+    if (kind == F_CENTRAL || kind == F_RUSANOV) {
+      double fm[NS], fp[NS];
+      const double wm = flux_ws_recip32<LAW, DIM>(L, d, qm, am, fm);
+      const double wp = flux_ws_recip32<LAW, DIM>(L, d, qp, ap, fp);
+#pragma unroll
+      for (int s = 0; s < NS; ++s) nf[s] = ((fm[s] + fp[s]) / 2.0) * sgn;
+      if (kind == F_RUSANOV) {
+        const float ws = (float)dmax(wm, wp);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) nf[s] = nf[s] - (double)(ws * (float)((qp[s] - qm[s]) / 2.0));
+      }
+      if constexpr (LAW == LAW_SW) {
+        if (L.swtopo) {  // non-conservative surface term g h- (b+ - b-)/2 n, FP64 (balance)
+          const double t = L.grav * qm[0] * (ap[0] - am[0]) / 2.0;
+          nf[1 + d] = nf[1 + d] + t * sgn;
+        }
+      }
+      return true;
+    }
+  }
+  return false;
+}
+
 // ------------------------------------------------------------ surface flux
 // normal n = sgn * e_d; nf = numerical flux . n (length NS)
 template <int LAW, int DIM, class T>

@@ -294,7 +294,7 @@ __device__ __forceinline__ int pair_index(int a, int b, int Nq) { return a * Nq 
 // one face-node task (face t / Nfp of direction D_, node t % Nfp): gather
 // the neighbour trace (or the boundary state), evaluate the numerical flux and
 // store it lifted into the face's shared-memory slot
-template <int LAW, int DIM, int NAM, int D_>
+template <int LAW, int DIM, int NAM, int D_, bool F32S = false>
 __device__ __forceinline__ void face_task(const TendArgs& A, const LawP& L, int sflux, int naux, int Nq, int Np,
                                           int Nfp, int e, int t, const double* sq, const double* sa, double* ss,
                                           double gid, double lift_end) {
@@ -329,7 +329,9 @@ __device__ __forceinline__ void face_task(const TendArgs& A, const LawP& L, int 
     for (int k = 0; k < NAM; ++k) ap[k] = am[k];
   }
   double nf[NS];
-  surface_flux<LAW, DIM>(L, sflux, D_, sgn, qm, am, qp, ap, nf);
+  bool done = false;
+  if constexpr (F32S) done = surface_flux32<LAW, DIM>(L, sflux, D_, sgn, qm, am, qp, ap, nf);
+  if (!done) surface_flux<LAW, DIM>(L, sflux, D_, sgn, qm, am, qp, ap, nf);
   const double lift = gid * lift_end;
 #pragma unroll
   for (int s = 0; s < NS; ++s) ss[(face * Nfp + j) * NS + s] = lift * nf[s];
@@ -352,6 +354,9 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
   constexpr int NPRE = NPre<LAW, DIM, VK>::v;
   constexpr int NAM = NAuxMax<LAW, DIM>::v;
   constexpr bool PAIRS = (VK == VK_EC || VK == VK_KG || VK == VK_EC32 || VK == VK_KG32);
+  // FP32-flux form: the explicit operator's surface flux in FP32 too (the
+  // fused linear operator keeps FP64, like the implicit solve)
+  constexpr bool F32S = (VK == VK_EC32 || VK == VK_KG32);
   constexpr int PR_IDX = (VK == VK_EC32) ? 2 : DIM + 2;  // p/rho in the own-node values
   constexpr int NPV = PAIRS ? NPairVals<LAW, DIM, VK>::v : 0;
   constexpr int NPVS = PAIRS ? NPairVals<LAW, DIM, VK>::stride : 0;
@@ -678,9 +683,9 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
       }
       const int t = 2 * dd * Nfp + tt;
       switch (dd) {
-        case 0: face_task<LAW, DIM, NAM, 0>(A, L, A.sflux, naux_nl, Nq, Np, Nfp, ef, t, sqe, sae, sse, __ldg(A.ginv + 3 * ef), lift_end); break;
-        case 1: if constexpr (DIM > 1) face_task<LAW, DIM, NAM, 1>(A, L, A.sflux, naux_nl, Nq, Np, Nfp, ef, t, sqe, sae, sse, __ldg(A.ginv + 3 * ef + 1), lift_end); break;
-        default: if constexpr (DIM > 2) face_task<LAW, DIM, NAM, 2>(A, L, A.sflux, naux_nl, Nq, Np, Nfp, ef, t, sqe, sae, sse, __ldg(A.ginv + 3 * ef + 2), lift_end); break;
+        case 0: face_task<LAW, DIM, NAM, 0, F32S>(A, L, A.sflux, naux_nl, Nq, Np, Nfp, ef, t, sqe, sae, sse, __ldg(A.ginv + 3 * ef), lift_end); break;
+        case 1: if constexpr (DIM > 1) face_task<LAW, DIM, NAM, 1, F32S>(A, L, A.sflux, naux_nl, Nq, Np, Nfp, ef, t, sqe, sae, sse, __ldg(A.ginv + 3 * ef + 1), lift_end); break;
+        default: if constexpr (DIM > 2) face_task<LAW, DIM, NAM, 2, F32S>(A, L, A.sflux, naux_nl, Nq, Np, Nfp, ef, t, sqe, sae, sse, __ldg(A.ginv + 3 * ef + 2), lift_end); break;
       }
     }
   }
