@@ -652,15 +652,19 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
 
   // ------------------------------------------------------------ faces
   // Face-node tasks of all elements of the CTA, spread over all its threads.
-  // Each direction's 2*Nfp tasks are padded to whole warps, so a warp only
-  // ever runs faces of one direction (the flux code is not split between
-  // directions inside a warp); the direction is dispatched to a compile-time
-  // constant so every state / normal index in the numerical flux is static.
+  // Where it costs little padding, each direction's 2*Nfp tasks are padded to
+  // whole warps, so a warp only runs faces of one direction (the flux code is
+  // not split between directions inside a warp); the direction is dispatched
+  // to a compile-time constant so every state / normal index in the numerical
+  // flux is static.
   {
     const double lift_end = sm[2 * Nq * Nq];
     const bool lin_faces = FUSE && LAW == LAW_EG && ((A.lin_dirs >> DZ) & 1);
     const int naux_nl = FUSE ? A.naux_nl : naux;
-    const int fp = ((2 * Nfp + 31) / 32) * 32;
+    // warp-aligned groups when that costs little padding (3-D N=3, 4, 7),
+    // else dense (small faces would leave most lanes idle)
+    const int fpad = ((2 * Nfp + 31) / 32) * 32;
+    const int fp = (10 * fpad <= 13 * 2 * Nfp) ? fpad : 2 * Nfp;
     const int per_elem = (DIM + (lin_faces ? 1 : 0)) * fp;
     for (int v = threadIdx.x; v < A.E * per_elem; v += blockDim.x) {
       const int es = v / per_elem, r = v - es * per_elem;
