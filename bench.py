@@ -117,13 +117,46 @@ def build_case(precision="fp64", K=16):
 
 
 def dist_init():
+    """One process per GPU (torchrun's RANK / WORLD_SIZE / MASTER_*): NCCL with
+    GPUs, gloo without (the CPU tests of this plumbing)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if world > 1:
+        import torch
         import torch.distributed as dist
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=timedelta(seconds=120))
         return dist, int(os.environ.get("RANK", "0")), world
     return None, 0, 1
+
+
+def max_over_ranks(x: float, dist) -> float:
+    """The largest of every rank's value (device times: the job takes as long
+    as its slowest rank)."""
+    if dist is None:
+        return float(x)
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x: float, dist) -> float:
+    """The sum of every rank's value (work done by independent replicas)."""
+    if dist is None:
+        return float(x)
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def instance_seeds(n_inst: int, rank: int):
+    """Seeds of one rank's independent instances (replicas: ranks share no
+    instance, so no data-path collective is needed)."""
+    return [1000 * (rank + 1) + i for i in range(n_inst)]
 
 
 # ----------------------------------------------------------- reference arm
@@ -268,10 +301,7 @@ def run_ours(args):
         nl, tm = _lib.C.c_long(), _lib.C.c_double()
         _lib.check(L.atb_profile_read(k, _lib.C.byref(nl), _lib.C.byref(tm)))
         prof[name] = {"launches": nl.value, "ms": tm.value}
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist)
     assert torch.isfinite(q).all(), "non-finite state after the timed steps"
 
     # ------------------------------------------------------------- e2e
@@ -295,10 +325,7 @@ def run_ours(args):
     e1.record(stream)
     barrier()
     ms_e2e = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ms_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    ms_e2e = max_over_ranks(ms_e2e, dist)
 
     if rank != 0:
         if dist is not None:
@@ -445,13 +472,15 @@ def run_serve(args):
         den = sum(float(np.sum(MJ * ref[s] ** 2)) for s in range(ref.shape[0]))
         errs.append(math.sqrt(num / den))
     srv.close()
+    span = max_over_ranks(st.makespan_s, dist)
+    total = sum_over_ranks(st.extra["dof_stage_updates"], dist)
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
         return 0
     lat = np.array([r.latency for r in reqs])
     line = {
-        "metric": "DOF-stage updates/s", "value": st.dof_stage_per_s * world, "unit": "DOF-stage/s",
+        "metric": "DOF-stage updates/s", "value": total / span, "unit": "DOF-stage/s",
         "n_gpus": world, "steps": int(sum(r.nsteps for r in reqs)), "warmup": args.warmup,
         "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64-state/f32-flux", "data": "synthetic",
@@ -595,6 +624,7 @@ def run_c5(args):
     with ClockSampler(torch.cuda.current_device()) as clk:
         q64, ms64, nl64, prof64 = run("fp64")
         q32, ms32, nl32, prof32 = run("fp32flux")
+    ms64, ms32 = max_over_ranks(ms64, dist), max_over_ranks(ms32, dist)
     assert torch.isfinite(q64).all() and torch.isfinite(q32).all(), "non-finite state"
 
     def wnorm2(a):
@@ -679,7 +709,7 @@ def run_swbatch(args):
 
     n_inst, K, N = args.instances, 32, 4
     steps = args.steps if args.steps is not None else 500
-    seeds = [1000 * (rank + 1) + i for i in range(n_inst)]
+    seeds = instance_seeds(n_inst, rank)
 
     def cases(precision, lake=False, n=n_inst):
         return [P.sw_fplane(N=N, K=K, seed=sd, precision=precision, lake_at_rest=lake, steps=steps)
@@ -732,6 +762,7 @@ def run_swbatch(args):
     e1.record()
     barrier()
     ms_seq = e0.elapsed_time(e1)
+    ms32, ms64, ms_seq = (max_over_ranks(x, dist) for x in (ms32, ms64, ms_seq))
     dofs_inst = dofs // n_inst
 
     # accuracy: per instance relative L2 (MJ-weighted) against the FP64 run
