@@ -122,6 +122,36 @@ def test_operator_apply(orc, case):
         assert err <= 1e-12, (case, inc, err)
 
 
+@pytest.mark.parametrize("law,form,sf", [("adv", "weak", "rusanov"), ("euler", "ec", "rusanov"),
+                                         ("euler", "kg", "roe"), ("sw", "ec", "rusanov")])
+@pytest.mark.parametrize("dim", [1, 2, 3])
+def test_single_element_periodic(orc, law, form, sf, dim):
+    """K = 1 per dimension: every face's neighbour is the element itself."""
+    dg = make_dg(law, dim, 3, 1, form, sf)
+    odg = orc.DGSEM(dg)
+    q = PT.random_state(dg)
+    dq_o = np.zeros_like(q)
+    odg(dq_o, q, 0.0, increment=False)
+    qd = PT.to_dev(q)
+    dqd = PT.to_dev(np.zeros_like(q))
+    dg(dqd, qd, 0.0, increment=False)
+    assert PT.rel_dof_error(PT.to_host(dqd), dq_o) <= 1e-12
+
+
+def test_stacked_ordering_matches_cartesian(orc):
+    """The stacked element ordering (vertical columns contiguous) gives the
+    oracle's operator too."""
+    dg = make_dg("euler", 3, 3, 3, "ec", "rusanov", ordering="stacked")
+    odg = orc.DGSEM(dg)
+    q = PT.random_state(dg)
+    dq_o = np.zeros_like(q)
+    odg(dq_o, q, 0.0, increment=False)
+    qd = PT.to_dev(q)
+    dqd = PT.to_dev(np.zeros_like(q))
+    dg(dqd, qd, 0.0, increment=False)
+    assert PT.rel_dof_error(PT.to_host(dqd), dq_o) <= 1e-12
+
+
 @pytest.mark.parametrize("kernel", ["per_dir", "per_dir_symmetric", "naive"])
 @pytest.mark.parametrize("dim", [2, 3])
 def test_fd_kernel_types(orc, kernel, dim):
