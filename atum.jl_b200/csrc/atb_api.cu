@@ -172,8 +172,8 @@ namespace {
 // warps (the face tasks are spread over warp-aligned groups)
 int cta_threads(int E, int Np) { return ((E * Np + 31) / 32) * 32; }
 
-size_t op_smem(const atb_op* op, int E) {
-  return tend_smem_bytes(op->ns, op->npre, op->naux_used, op->dim, op->Nq, op->Np, op->Nfp, E, op->npv);
+size_t op_smem(const atb_op* op, int E, int pf = 0) {
+  return tend_smem_bytes(op->ns, op->npre, op->naux_used, op->dim, op->Nq, op->Np, op->Nfp, E, op->npv, false, pf);
 }
 
 void fill_args(const atb_op* op, TendArgs& A) {
@@ -203,6 +203,7 @@ void fill_args(const atb_op* op, TendArgs& A) {
   A.lin_sflux = 0;
   A.lin_dirs = 0;
   A.naux_nl = op->naux_used;
+  A.pf = 0;
 }
 
 // EPI_ARK accumulators of one stage (see atb_tendency.cuh)
@@ -234,11 +235,12 @@ int run_tendency(atb_op* op, int epi, const double* const* q, double* const* out
     A.out[s] = out ? out[s < op->ns ? s : 0] : nullptr;
     A.out2[s] = out2 ? out2[s < op->ns ? s : 0] : nullptr;
   }
+  const size_t smem = op->smem;  // plain kernels: no epilogue prefetch (A.pf = 0)
   int grid = (op->K_active + op->E - 1) / op->E;
   if (grid == 0) return ATB_OK;
   {
     ProfScope ps(op->prof_class, st);
-    op->launch(A, grid, cta_threads(op->E, op->Np), op->smem, st);
+    op->launch(A, grid, cta_threads(op->E, op->Np), smem, st);
   }
   return check_launch("tendency");
 }
@@ -1195,14 +1197,20 @@ int run_fused(atb_solver* s, double* const* Q, const ArkAcc& ark, cudaStream_t s
   const int naux = op->dim + 3;  // [Phi, grad Phi, rho_ref, p_ref] staged for both operators
   A.naux = naux;
   int E = op->E;
+  int pf = 0;
+  for (int j = 0; j < 3; ++j) pf += (ark.acc[j][0] && ark.accin[j][0]) ? 1 : 0;
   auto bytes = [&](int e) {
-    return tend_smem_bytes(op->ns, op->npre, naux, op->dim, op->Nq, op->Np, op->Nfp, e, op->npv, true);
+    return tend_smem_bytes(op->ns, op->npre, naux, op->dim, op->Nq, op->Np, op->Nfp, e, op->npv, true, pf);
   };
   // fused kernels are compiled for fused_max_threads per CTA
   const int maxthr = fused_max_threads(op->Nq);
   while (E > 1 && (cta_threads(E, op->Np) > maxthr || bytes(E) > 100 * 1024)) --E;
   if (cta_threads(E, op->Np) > maxthr) return fail(ATB_ERR_INVALID, "element too large for the fused ARK stage kernel");
+  if (pf && bytes(E) > 227 * 1024) {
+    pf = 0;  // no room: the epilogue reads its accumulators directly
+  }
   A.E = E;
+  A.pf = pf;
   A.epi = EPI_ARK;
   A.lin_law = s->lin->law;
   A.lin_sflux = s->lin->sflux;

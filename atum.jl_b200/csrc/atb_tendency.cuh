@@ -44,6 +44,11 @@
 
 namespace atb {
 
+__device__ __forceinline__ void tend_cp_async8(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
 // VK_EC32: the entropy-conservative volume flux in the FP32-flux precision
 // form (mixed: balance-critical terms in FP64 adds/multiplies, the rest FP32)
 // VK_KG32: the Kennedy-Gruber volume flux in the FP32-flux precision form
@@ -75,6 +80,7 @@ struct TendArgs {
   LawP lin_law;
   int lin_sflux, lin_dirs;
   int naux_nl;  // aux components the explicit operator's faces read (fused launches stage more)
+  int pf;       // epilogue input fields prefetched into shared memory (0: read at the end)
   size_t stride;      // K*Np
   const double* q[5];
   double* out[5];
@@ -111,11 +117,12 @@ template <int LAW, int DIM, int VK> struct NPairVals {
 };
 
 inline size_t tend_smem_bytes(int ns, int npre, int naux, int dim, int Nq, int Np, int Nfp, int E, int npvs,
-                              bool fuse = false) {
+                              bool fuse = false, int pf = 0) {
   const int npl = Nq * (Nq - 1) / 2;
   size_t per = (size_t)(ns + naux + npre) * Np + (size_t)2 * dim * Nfp * ns;
   if (npvs > 0) per += (size_t)Nfp * npl * npvs;
   if (fuse) per += (size_t)ns * Np + (size_t)2 * Nfp * ns;  // linear flux rows, linear face slots
+  per += (size_t)pf * ns * Np;                              // prefetched epilogue inputs
   return sizeof(double) * (2 * (size_t)Nq * Nq + 2 + per * E) + 64 * sizeof(int);
 }
 
@@ -375,7 +382,7 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
   double* sC = sm;            // Cfd
   double* sW = sm + Nq * Nq;  // Cw
   const size_t slotsz = (size_t)(NS + naux + NPRE) * Np + (size_t)2 * DIM * Nfp * NS + (size_t)Nfp * npl * NPVS +
-                        (FUSE ? (size_t)NS * Np + (size_t)2 * Nfp * NS : 0);
+                        (FUSE ? (size_t)NS * Np + (size_t)2 * Nfp * NS : 0) + (size_t)A.pf * NS * Np;
   double* sq = sm + tabn + slot * slotsz;
   double* sa = sq + NS * Np;
   double* sp = sa + naux * Np;
@@ -383,6 +390,8 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
   double* spv = ss + 2 * DIM * Nfp * NS;  // pair values
   double* slf = spv + (size_t)Nfp * npl * NPVS;  // FUSE: linear vertical flux per node
   double* ssl = slf + NS * Np;                   // FUSE: linear z-face slots
+  // prefetched epilogue inputs: the last A.pf*NS*Np doubles of the slot
+  double* spf_in = sq + slotsz - (size_t)A.pf * NS * Np;
   int* spair = (int*)(sm + tabn + A.E * slotsz);
   for (int t = threadIdx.x; t < tabn; t += blockDim.x) sm[t] = A.tab[t];
   if (PAIRS && threadIdx.x < npl) {
@@ -392,6 +401,36 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
   }
   const LawP& L = A.law;
   const size_t gid = (size_t)e * Np + node;
+  // Fused ARK stages: the epilogue's own-node inputs (the accumulators) are
+  // copied into shared memory now, asynchronously, so their latency hides
+  // behind the whole tendency; each thread later reads only what it copied.
+  // (Plain kernels keep reading them at the end: the extra code costs them
+  // registers, measured slower.)
+  if (FUSE && A.pf > 0 && act) {
+    int j = 0;
+    auto pf5 = [&](const double* p0, const double* p1, const double* p2, const double* p3, const double* p4) {
+      const double* P[5] = {p0, p1, p2, p3, p4};
+#pragma unroll
+      for (int s = 0; s < NS; ++s) tend_cp_async8(spf_in + (j * NS + s) * Np + node, P[s] + gid);
+      ++j;
+    };
+    switch (A.epi) {
+      case EPI_ADD: pf5(A.out[0], A.out[1], A.out[2], A.out[3], A.out[4]); break;
+      case EPI_LSRK:
+        if (A.a != 0.0) pf5(A.out[0], A.out[1], A.out[2], A.out[3], A.out[4]);
+        break;
+      case EPI_ARK:
+        if (!FUSE) pf5(A.out[0], A.out[1], A.out[2], A.out[3], A.out[4]);
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+          if (A.acc[k][0] && A.accin[k][0])
+            pf5(A.accin[k][0], A.accin[k][1], A.accin[k][2], A.accin[k][3], A.accin[k][4]);
+        break;
+      case EPI_SUBOUT2:
+      case EPI_RLSRK: pf5(A.out2[0], A.out2[1], A.out2[2], A.out2[3], A.out2[4]); break;
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  }
   double qn[NS], an[NAM], Pn[NPRE > 0 ? NPRE : 1];
 #pragma unroll
   for (int k = 0; k < NAM; ++k) an[k] = 0.0;
@@ -716,6 +755,10 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
   }
 
   // --------------------------------------------------------- epilogue
+  const bool pfon = FUSE && A.pf > 0;
+  if (pfon) asm volatile("cp.async.wait_all;\n" ::: "memory");
+  // j-th prefetched field, state s (own node); the same order as issued
+  auto pin = [&](int j, int s) { return spf_in[(j * NS + s) * Np + node]; };
   switch (A.epi) {
     case EPI_SET:
 #pragma unroll
@@ -723,7 +766,7 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
       break;
     case EPI_ADD:
 #pragma unroll
-      for (int s = 0; s < NS; ++s) A.out[s][gid] = A.out[s][gid] + T[s];
+      for (int s = 0; s < NS; ++s) A.out[s][gid] = (pfon ? pin(0, s) : A.out[s][gid]) + T[s];
       break;
     case EPI_LSRK: {
       const double bdt = A.dte ? A.bdt * A.dte[e] : A.bdt;
@@ -731,7 +774,7 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
       for (int s = 0; s < NS; ++s) {
         // first stage (a = 0): the previous increment is not read, so stale
         // or never-written increment storage cannot leak into the step
-        const double dqn = (A.a != 0.0) ? A.a * A.out[s][gid] + T[s] : T[s];
+        const double dqn = (A.a != 0.0) ? A.a * (pfon ? pin(0, s) : A.out[s][gid]) + T[s] : T[s];
         A.out[s][gid] = dqn;
         A.out2[s][gid] = qn[s] + bdt * dqn;
       }
@@ -740,12 +783,14 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
         // fused: T = N(Q), TL = L(Q); else out holds N(Q) and T = L(Q)
-        const double E = FUSE ? T[s] - TL[s] : A.out[s][gid] - T[s];
+        const double E = FUSE ? T[s] - TL[s] : (pfon ? pin(0, s) : A.out[s][gid]) - T[s];
         const double I = FUSE ? TL[s] : T[s];
+        int jj = FUSE ? 0 : 1;
 #pragma unroll
         for (int j = 0; j < 3; ++j)
           if (A.acc[j][0]) {
-            const double base = A.accin[j][0] ? A.accin[j][s][gid] : qn[s];
+            double base = qn[s];
+            if (A.accin[j][0]) base = pfon ? pin(jj++, s) : A.accin[j][s][gid];
             A.acc[j][s][gid] = base + A.adt * (A.ca[j] * E + A.cb[j] * I);
           }
       }
@@ -753,15 +798,17 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
     case EPI_SUBOUT2:
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
+        const double o2 = pfon ? pin(0, s) : A.out2[s][gid];
         A.out[s][gid] = T[s];
-        A.out2[s][gid] = A.out2[s][gid] - T[s];
+        A.out2[s][gid] = o2 - T[s];
       }
       break;
     case EPI_RLSRK:
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
+        const double o2 = pfon ? pin(0, s) : A.out2[s][gid];
         A.out[s][gid] = T[s];
-        A.out2[s][gid] = A.a * A.out2[s][gid] + T[s];
+        A.out2[s][gid] = A.a * o2 + T[s];
       }
       break;
   }
