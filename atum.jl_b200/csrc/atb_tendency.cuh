@@ -618,10 +618,11 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
       if (act) {
         const int line = (d == 0) ? node / Nq : (d == 1) ? ijk[0] + Nq * ijk[2] : node % (Nq * Nq);
         const double* lp = spv + (size_t)line * npl * NPVS;
+        // the Nq - 1 partners m != id, without a skipped (divergent) iteration
 #pragma unroll
-        for (int m = 0; m < (CQ ? NQ_ : 8); ++m) {
-          if (!CQ && m >= Nq) break;
-          if (m == id) continue;
+        for (int k = 0; k < (CQ ? NQ_ - 1 : 7); ++k) {
+          if (!CQ && k >= Nq - 1) break;
+          const int m = k + (k >= id ? 1 : 0);
           const int p = (m < id) ? pair_index(m, id, Nq) : pair_index(id, m, Nq);
           const double* fv = lp + p * NPVS;
           double f[NS];
