@@ -63,19 +63,21 @@ template <class T> __device__ __forceinline__ T logavg(T a, T b) {
 }
 
 // Logarithmic mean for the flux-differencing volume term: the reference's
-// series is used below u = f^2 = ((a-b)/(a+b))^2 < 1e-4 (five terms, truncation
-// error below u^5/11 < 1e-20 relative), so log() is evaluated only for
-// neighbouring values more than ~2% apart; above the threshold
-// (a - b) / log(a / b) is accurate to a few ulps because |log(a/b)| > 0.02.
+// series, extended to eight terms, is used below u = f^2 = ((a-b)/(a+b))^2 <
+// 1e-2 (truncation error below u^8/17 < 1e-17 relative), so log() is
+// evaluated only for values more than ~20% apart; above the threshold
+// (a - b) / log(a / b) is accurate to a few ulps because |log(a/b)| > 0.2.
 // (Same function as the reference's logavg to FP64 rounding; the threshold
 // follows Ranocha et al., "Efficient implementation of modern entropy stable
 // and kinetic energy preserving DG methods", 2022.)
 template <class T> __device__ __forceinline__ T logavg_fast(T a, T b) {
   const T s = a + b, d = a - b;
-  if (d * d < T(1e-4) * (s * s)) {
+  if (d * d < T(1e-2) * (s * s)) {
+    // eight series terms: truncation under 1e-17 relative below u = 1e-2
     const T f = d / s;
     const T u = f * f;
-    const T F = T(1) + u * (T(1) / T(3) + u * (T(1) / T(5) + u * (T(1) / T(7) + u * (T(1) / T(9)))));
+    const T F = T(1) + u * (T(1) / T(3) + u * (T(1) / T(5) + u * (T(1) / T(7) + u * (T(1) / T(9) +
+                u * (T(1) / T(11) + u * (T(1) / T(13) + u * (T(1) / T(15))))))));
     return s / (T(2) * F);
   }
   return d / dlog(a / b);

@@ -131,20 +131,26 @@ __host__ __device__ constexpr int ipow(int b, int e) { return e == 0 ? 1 : b * i
 // volume-term two-point fluxes on the staged per-node layouts (row d)
 //
 // EC flux: when both logarithmic means are on their series branch
-// (u = ((a-b)/(a+b))^2 < 1e-4 for rho and for b, the common case between
-// neighbouring nodes of a resolved flow) every division of the flux shares
-// ONE reciprocal, 1/((r1+r2)^2 (b1+b2)^2):
+// (u = ((a-b)/(a+b))^2 < 1e-2 for rho and for b, the common case between
+// the nodes of an element of a resolved flow) every division of the flux
+// shares ONE reciprocal, 1/((r1+r2)^2 (b1+b2)^2):
 //   rho_log = (r1+r2)/2 * G(u_rho),  b_log = (b1+b2)/2 * G(u_b),
 //   rho_avg/(2 b_avg) = (r1+r2)/2 / (b1+b2),
 //   1/(2 (gamma-1) b_log) = F(u_b) / ((gamma-1) (b1+b2)),
-// with F(u) = 1 + u/3 + u^2/5 + u^3/7 + u^4/9 (the reference's series) and
-// G = 1/F = 1 - u/3 - 4u^2/45 - 44u^3/945 - 428u^4/14175 (truncation below
-// 3e-22 relative for u < 1e-4).  Otherwise the general form below is used.
+// with F(u) = 1 + u/3 + u^2/5 + ... + u^7/15 (the reference's series, longer)
+// and G = 1/F to the same order (truncation below 1e-17 relative for
+// u < 1e-2).  Otherwise the general form below is used.  A wide series range
+// keeps the pairs of a warp on one branch.
+// F(u) = atanh(sqrt u) / sqrt u = sum_k u^k / (2k+1) and G = 1 / F, eight
+// terms each: below u = 1e-2 the truncation is under 1e-17 relative, so the
+// series branch is as accurate as the logarithm it replaces there
 template <class T> __device__ __forceinline__ T series_F(T u) {
-  return T(1) + u * (T(1) / T(3) + u * (T(1) / T(5) + u * (T(1) / T(7) + u * (T(1) / T(9)))));
+  return T(1) + u * (T(1) / T(3) + u * (T(1) / T(5) + u * (T(1) / T(7) + u * (T(1) / T(9) +
+         u * (T(1) / T(11) + u * (T(1) / T(13) + u * (T(1) / T(15))))))));
 }
 template <class T> __device__ __forceinline__ T series_G(T u) {
-  return T(1) - u * (T(1) / T(3) + u * (T(4) / T(45) + u * (T(44) / T(945) + u * (T(428) / T(14175)))));
+  return T(1) - u * (T(1) / T(3) + u * (T(4) / T(45) + u * (T(44) / T(945) + u * (T(428) / T(14175) +
+         u * (T(10196) / T(467775) + u * (T(10719068) / T(638512875) + u * (T(25865068) / T(1915538625))))))));
 }
 
 template <int LAW, int DIM, class T>
@@ -160,7 +166,7 @@ __device__ __forceinline__ void ec_vol(T gamma, T igm1, int d, T r1, const T* P1
   const T rs = r1 + r2, rd = r1 - r2, bs = b1 + b2, bd = b1 - b2;
   const T rs2 = rs * rs, bs2 = bs * bs, rd2 = rd * rd, bd2 = bd * bd;
   T rho_log, pc, cterm;
-  if (rd2 < T(1e-4) * rs2 && bd2 < T(1e-4) * bs2) {
+  if (rd2 < T(1e-2) * rs2 && bd2 < T(1e-2) * bs2) {
     const T inv = T(1) / (rs2 * bs2);
     const T ur = rd2 * bs2 * inv, ub = bd2 * rs2 * inv;
     const T inv_bs = bs * rs2 * inv;  // 1 / (b1 + b2)
