@@ -217,14 +217,15 @@ __device__ __forceinline__ void ec_vol32(float igm1, int d, double r1, double p1
   const float ur = fr * fr, ub = fb * fb;
   double rho_log;
   float cterm;
-  if (ur < 1e-4f && ub < 1e-4f) {
-    // 1 - G(u) = u/3 + 4u^2/45 + 44u^3/945 + ...
-    const float cr = ur * (1.f / 3.f + ur * (4.f / 45.f + ur * (44.f / 945.f)));
+  if (ur < 1e-2f && ub < 1e-2f) {
+    // 1 - G(u) = u/3 + 4u^2/45 + 44u^3/945 + ... (the terms of series_G)
+    const float cr = ur * (1.f / 3.f + ur * (4.f / 45.f + ur * (44.f / 945.f + ur * (428.f / 14175.f +
+                     ur * (10196.f / 467775.f + ur * (10719068.f / 638512875.f + ur * (25865068.f / 1915538625.f)))))));
     rho_log = rho_avg - rho_avg * (double)cr;
     cterm = series_F(ub) * igm1 / bs;  // 1 / (2 (gamma-1) b_log)
   } else {
     rho_log = logavg_fast(r1, r2);
-    const float b_log = (ub < 1e-4f) ? 0.5f * bs * series_G(ub) : bd / logf((float)b1 / (float)b2);
+    const float b_log = (ub < 1e-2f) ? 0.5f * bs * series_G(ub) : bd / logf((float)b1 / (float)b2);
     cterm = 0.5f * igm1 / b_log;
   }
   const double corr = (double)((float)(p1 - p2) * (float)(b2 - b1) / (2.f * bs));
