@@ -672,28 +672,17 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
     }
   }
 
-  // ------------------------------------ fused linear operator (volume)
-  // the weak-form linear Euler-gravity operator along z, evaluated exactly as
-  // its own launch would: sources, then the D^T contraction of the staged
-  // flux rows, then (below) the z faces
   constexpr int DZ = DIM - 1;
-  double TL[NS];
+  // While the face tasks run (the register-heaviest part), the explicit
+  // accumulators wait in the pair buffer (free after the last direction) and
+  // the own-node state and aux are re-read from their staged copies
+  // afterwards: nothing of this node's stays live in registers across them.
+  constexpr bool PARK = PAIRS && CQ && ((size_t)ipow(NQ_ > 0 ? NQ_ : 1, DIM - 1) * ((NQ_ * (NQ_ - 1)) / 2) * NPVS >=
+                                        (size_t)NS * ipow(NQ_ > 0 ? NQ_ : 1, DIM));
+  if constexpr (PARK) {
+    if (act) {
 #pragma unroll
-  for (int s = 0; s < NS; ++s) TL[s] = 0.0;
-  if constexpr (FUSE && LAW == LAW_EG) {
-    if (act && ((A.lin_dirs >> DZ) & 1)) {
-      add_sources<LAW_LEG, DIM>(A.lin_law, true, qn, an, TL);
-      const int sd = (DZ == 0) ? 1 : (DZ == 1) ? Nq : Nq * Nq;
-      const int id = ijk[DZ];
-      const int base = node - id * sd;
-#pragma unroll
-      for (int m = 0; m < (CQ ? NQ_ : 8); ++m) {
-        if (!CQ && m >= Nq) break;
-        const int nn = base + m * sd;
-        const double c = sW[id * Nq + m] * gi[DZ];
-#pragma unroll
-        for (int s = 0; s < NS; ++s) TL[s] = TL[s] + c * slf[s * Np + nn];
-      }
+      for (int s = 0; s < NS; ++s) spv[s * Np + node] = T[s];
     }
   }
 
@@ -742,6 +731,16 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
   }
   __syncthreads();
   if (!act) return;
+  if constexpr (PARK) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      T[s] = spv[s * Np + node];
+      qn[s] = sq[s * Np + node];
+    }
+#pragma unroll
+    for (int k = 0; k < NAM; ++k)
+      if (k < naux) an[k] = sa[k * Np + node];
+  }
 #pragma unroll
   for (int d = 0; d < DIM; ++d) {
     if (!((A.dirs >> d) & 1)) continue;
@@ -752,7 +751,28 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
 #pragma unroll
     for (int s = 0; s < NS; ++s) T[s] = T[s] - ss[(face * Nfp + j) * NS + s];
   }
+  // fused linear operator: the weak-form linear Euler-gravity operator along
+  // z, evaluated exactly as its own launch would: sources, then the D^T
+  // contraction of the staged flux rows, then the z faces
+  double TL[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) TL[s] = 0.0;
   if constexpr (FUSE && LAW == LAW_EG) {
+    if ((A.lin_dirs >> DZ) & 1) {
+      add_sources<LAW_LEG, DIM>(A.lin_law, true, qn, an, TL);
+      const int sd = (DZ == 0) ? 1 : (DZ == 1) ? Nq : Nq * Nq;
+      const int id = ijk[DZ];
+      const int base = node - id * sd;
+      const double gz = __ldg(A.ginv + 3 * e + DZ);
+#pragma unroll
+      for (int m = 0; m < (CQ ? NQ_ : 8); ++m) {
+        if (!CQ && m >= Nq) break;
+        const int nn = base + m * sd;
+        const double c = sW[id * Nq + m] * gz;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) TL[s] = TL[s] + c * slf[s * Np + nn];
+      }
+    }
     const int id = ijk[DZ];
     if (((A.lin_dirs >> DZ) & 1) && (id == 0 || id == Nq - 1)) {
       const int side = (id == Nq - 1) ? 1 : 0;
