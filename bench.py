@@ -12,6 +12,10 @@ the batched banded column solve.  One step = one ARK23 step = 3 stages; one
 DOF-stage = one conserved variable at one node through one stage.  Inputs are
 synthetic (seeded, built on the host), no dataset.
 
+--scheme lsrk54   the same bubble stepped fully explicitly by LSRK54 (5 stages
+                  per step, each one tendency launch with the register update
+                  in its epilogue) instead of IMEX ARK23
+
 --impl ours       the CUDA library through the C ABI (default)
 --impl reference  the reference's CPU algorithm: the C++ oracle port (the
                   Julia reference cannot run on this image), all host cores,
@@ -111,9 +115,32 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_case(precision="fp64", K=16):
+SCHEME_STAGES = {"ark23": 3, "lsrk54": 5}
+
+
+def build_case(precision="fp64", K=16, scheme="ark23"):
+    """The rising bubble: IMEX ARK23 with the vertical acoustics implicit, or
+    the fully explicit LSRK54 run of the same problem at its smaller dt."""
     import problems as P
-    return P.bubble_3d(N=4, K=K, imex=True, steps=200, precision=precision)
+    return P.bubble_3d(N=4, K=K, imex=(scheme == "ark23"), steps=200, precision=precision)
+
+
+def make_solver(A, case, q, scheme):
+    if scheme == "ark23":
+        return A.ARK23(case.dg, case.lindg, q, case.dt, split_rhs=False)
+    return A.LSRK54(case.dg, q, case.dt)
+
+
+def make_oracle_solver(orc, case, q, scheme):
+    dg = orc.DGSEM(case.dg)
+    if scheme == "ark23":
+        return orc.ARK23(dg, orc.DGSEM(case.lindg), q, case.dt, split_rhs=False)
+    return orc.LSRK54(dg, q, case.dt)
+
+
+def scheme_label(scheme):
+    return ("IMEX ARK23 split_rhs=false, vertical banded solve" if scheme == "ark23"
+            else "explicit LSRK54 (Carpenter-Kennedy 5-stage)")
 
 
 def dist_init():
@@ -169,24 +196,23 @@ def run_reference(args):
     load_pkg()
     threads = os.cpu_count() or 1
     orc.set_threads(threads)
-    case = build_case_sample()
-    dg = orc.DGSEM(case.dg)
-    lin = orc.DGSEM(case.lindg)
+    case = build_case_sample(args.scheme)
     q = case.q0.copy()
-    s = orc.ARK23(dg, lin, q, case.dt, split_rhs=False)
+    s = make_oracle_solver(orc, case, q, args.scheme)
     dofs = q.size
     s.step(q, args.warmup)
     t0 = time.perf_counter()
     s.step(q, args.steps)
     T = time.perf_counter() - t0
-    v = dofs * 3 * args.steps / T
+    v = dofs * SCHEME_STAGES[args.scheme] * args.steps / T
     sample = (f"{case.dg.grid.Kd[0]}x{case.dg.grid.Kd[1]}x{case.dg.grid.Kd[2]} elements (a horizontal "
-              f"sub-sample of the 16x16x16 workload, same columns), {dofs} DOFs, ARK23 steps")
+              f"sub-sample of the 16x16x16 workload, same columns), {dofs} DOFs, "
+              f"{args.scheme.upper()} steps")
     line = {"metric": "DOF-stage updates/s", "value": v, "unit": "DOF-stage/s", "n_gpus": 0, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": T / args.steps * 1e3, "higher_is_better": True,
             "impl": "reference", "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "3-D Euler-gravity rising bubble, 16^3 hexahedra, N=4, FP64, IMEX ARK23 "
-                                   "(CPU: horizontal sub-sample)", "sample": sample},
+            "config": {"workload": f"3-D Euler-gravity rising bubble, 16^3 hexahedra, N=4, FP64, "
+                                   f"{scheme_label(args.scheme)} (CPU: horizontal sub-sample)", "sample": sample},
             "cpu_baseline": {"value": v, "unit": "DOF-stage/s", "cores": threads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": v, "unit": "DOF-stage/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -195,13 +221,13 @@ def run_reference(args):
     return 0
 
 
-def build_case_sample():
+def build_case_sample(scheme="ark23"):
     """Horizontal sub-sample of the benchmark workload: 4x4 of the 16x16
     element columns at full height, identical spacing, physics and dt."""
     import numpy as np
     import problems as P
     import atum_b200 as A
-    full = build_case()
+    full = build_case(scheme=scheme)
     L = 10e3
     K = 16
     v = np.array([L * i / K for i in range(K + 1)])
@@ -224,29 +250,30 @@ def build_case_sample():
     rho = p / (R * theta * pi_ex)
     z = np.zeros_like(rho)
     q0 = np.ascontiguousarray(np.stack([rho, z, z, z, law.energy(rho, [z, z, z], p, aux[0])]))
+    if scheme != "ark23":
+        return P.Case("bubble_3d_sample", dg, q0, full.dt, full.timeend)
     return P.Case("bubble_3d_sample", dg, q0, full.dt, full.timeend, solver="ARK23", lindg=lin, split_rhs=False,
                   adjust_final=False)
 
 
-def cpu_baseline_sample():
-    """Oracle port on the host cores: one ARK23 step of the horizontal sub-sample."""
+def cpu_baseline_sample(scheme="ark23"):
+    """Oracle port on the host cores: two steps of the horizontal sub-sample."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as orc
     threads = os.cpu_count() or 1
     orc.set_threads(threads)
-    case = build_case_sample()
-    dg = orc.DGSEM(case.dg)
-    lin = orc.DGSEM(case.lindg)
+    case = build_case_sample(scheme)
     q = case.q0.copy()
-    s = orc.ARK23(dg, lin, q, case.dt, split_rhs=False)
+    s = make_oracle_solver(orc, case, q, scheme)
     s.step(q, 1)
     n = 2
     t0 = time.perf_counter()
     s.step(q, n)
     T = time.perf_counter() - t0
-    return {"value": q.size * 3 * n / T, "unit": "DOF-stage/s", "cores": threads, "kind": "port",
-            "sample": f"{n} ARK23 steps of a 4x4x16-element horizontal sub-sample ({q.size} DOFs) of the same "
-                      f"workload, {threads} threads"}
+    return {"value": q.size * SCHEME_STAGES[scheme] * n / T, "unit": "DOF-stage/s", "cores": threads,
+            "kind": "port",
+            "sample": f"{n} {scheme.upper()} steps of a 4x4x16-element horizontal sub-sample ({q.size} DOFs) of "
+                      f"the same workload, {threads} threads"}
 
 
 # ---------------------------------------------------------------- our arm
@@ -260,12 +287,16 @@ def run_ours(args):
     A = load_pkg()
     from atum_b200 import _lib
 
-    case = build_case(args.precision)
+    scheme = args.scheme
+    stages = SCHEME_STAGES[scheme]
+    case = build_case(args.precision, scheme=scheme)
     dofs = case.q0.size
     q = torch.as_tensor(case.q0, device="cuda").contiguous()
     # launch shapes picked by the library's autotuner (results do not depend on them)
-    tuned = {"tendency": A.batch.autotune(case.dg, q), "tendency_linear": A.batch.autotune(case.lindg, q)}
-    solver = A.ARK23(case.dg, case.lindg, q, case.dt, split_rhs=False)
+    tuned = {"tendency": A.batch.autotune(case.dg, q)}
+    if scheme == "ark23":
+        tuned["tendency_linear"] = A.batch.autotune(case.lindg, q)
+    solver = make_solver(A, case, q, scheme)
     L = _lib.lib()
     stream = torch.cuda.current_stream()
 
@@ -310,7 +341,7 @@ def run_ours(args):
     qh = torch.empty(case.q0.shape, dtype=torch.float64, pin_memory=True)
     qh.copy_(torch.as_tensor(case.q0))
     qd = torch.empty_like(q)
-    s2 = A.ARK23(case.dg, case.lindg, qd, case.dt, split_rhs=False)
+    s2 = make_solver(A, case, qd, scheme)
     ke = max(3, min(args.steps, 50))
     qd.copy_(qh, non_blocking=True)
     s2.step(qd, 1)
@@ -332,13 +363,13 @@ def run_ours(args):
             dist.destroy_process_group()
         return 0
 
-    value = world * dofs * 3 * args.steps / (ms * 1e-3)
-    e2e = world * dofs * 3 * ke / (ms_e2e * 1e-3)
+    value = world * dofs * stages * args.steps / (ms * 1e-3)
+    e2e = world * dofs * stages * ke / (ms_e2e * 1e-3)
     tend = prof["tendency"]
     avg_ms = tend["ms"] / max(1, tend["launches"])
     # the stage kernel: explicit EC tendency fused with the linear vertical
     # operator when the solver fuses them (no separate linear launches)
-    fused = prof["tendency_linear"]["launches"] == 0
+    fused = scheme == "ark23" and prof["tendency_linear"]["launches"] == 0
     flops_dof = FLOPS_PER_DOF_STAGE["bubble_3d_N4_ec_rusanov"]
     if fused:
         flops_dof += FLOPS_PER_DOF_STAGE["bubble_3d_N4_linear_weak_z"]
@@ -350,16 +381,19 @@ def run_ours(args):
     # algorithmic bytes per launch: fused stage kernel, averaged over the three
     # stages: Q (5) and aux (6) read; accumulators 15 written (stage 1), 10 read
     # + 10 written (stage 2), 5 read + 5 written (stage 3) -> 26 x 8 B per node.
-    # Unfused explicit tendency: Q (5), Phi (1) read, N(Q) (5) written.
-    bytes_launch = (26 if fused else 11) * 8 * dofs // 5
+    # LSRK54 stage kernel (tendency + register update in its epilogue): Q (5)
+    # and Phi (1) read, dQ read (5, stages 2-5), dQ and Q written (10) -> 20 on
+    # average.  Unfused ARK explicit tendency: Q (5), Phi (1) read, N(Q) (5)
+    # written.
+    bytes_launch = (26 if fused else 20 if scheme == "lsrk54" else 11) * 8 * dofs // 5
     line = {
         "metric": "DOF-stage updates/s", "value": value, "unit": "DOF-stage/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64-state/f32-flux",
         "data": "synthetic",
         "config": {"workload": "3-D Euler-gravity rising bubble, 16^3 hexahedra, N=4 (2,560,000 DOFs), EC volume + "
-                               "Rusanov surface flux, IMEX ARK23 split_rhs=false, vertical banded solve",
-                   "dofs": dofs, "stages_per_step": 3, "precision": args.precision,
+                               "Rusanov surface flux, " + scheme_label(scheme),
+                   "dofs": dofs, "stages_per_step": stages, "precision": args.precision,
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                    "l2": "working set ~0.21 GB > 126 MB L2 (no flush)",
                    "elements_per_cta": tuned},
@@ -369,7 +403,9 @@ def run_ours(args):
         "roofline": {"bound": "fp64",
                      "kernel": ("tendency_kernel<EulerGravity,3,EC,Nq=5,fused> (ARK23 stage: EC tendency + linear "
                                 "vertical operator)") if fused else
-                               "tendency_kernel<EulerGravity,3,EC,Nq=5> (explicit stage tendency)",
+                               ("tendency_kernel<EulerGravity,3,EC,Nq=5> (LSRK54 stage: tendency + register "
+                                "update)" if scheme == "lsrk54" else
+                                "tendency_kernel<EulerGravity,3,EC,Nq=5> (explicit stage tendency)"),
                      "flops_per_dof_stage": flops_dof,
                      "achieved": tflops, "peak": peak_fp64.value, "unit": "TFLOP/s",
                      "frac": tflops / peak_fp64.value if peak_fp64.value > 0 else None,
@@ -386,7 +422,7 @@ def run_ours(args):
         "clocks": clk.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sample()
+        line["cpu_baseline"] = cpu_baseline_sample(scheme)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -842,6 +878,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32flux"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scheme", default="ark23", choices=sorted(SCHEME_STAGES),
+                    help="time stepper of the bubble workload: IMEX ARK23 (default) or the fully explicit LSRK54 "
+                         "run of the same problem")
     ap.add_argument("--workload", default="bubble", choices=["bubble", "swbatch", "serve", "c5"],
                     help="bubble: 3-D rising bubble, IMEX ARK23 (default); swbatch: packed shallow-water "
                          "instances; serve: Poisson request stream through the serving loop; c5: 128x128x32 "
