@@ -888,6 +888,7 @@ struct atb_solver {
   int* d_e0 = nullptr;
   double* band = nullptr;
   double* blk = nullptr;
+  double* frag = nullptr;
   int ld = 0;
   // ARK23 stages fused into one kernel per stage (explicit tendency + linear
   // operator), when the two operators allow it (atb_solver_fuse)
@@ -911,6 +912,7 @@ void solver_free(atb_solver* s) {
   cudaFree(s->d_e0);
   cudaFree(s->band);
   cudaFree(s->blk);
+  cudaFree(s->frag);
   if (s->own_dte) cudaFree(s->d_dte);
   delete s;
 }
@@ -1033,6 +1035,15 @@ int build_band(atb_solver* s, cudaStream_t st) {
     const int BW1 = M.bw + 1;
     if ((rc = dalloc(&s->blk, (size_t)M.KV * 4 * BW1 * BW1))) return rc;
     launch_block_prep(s->band, M.KV, BW1, s->blk, st);
+    // the tile-sparse warp-owned solve, when the blocks have its zero structure
+    // (vertical coupling through face nodes only)
+    std::vector<double> hblk((size_t)M.KV * 4 * BW1 * BW1);
+    CK(cudaMemcpyAsync(hblk.data(), s->blk, hblk.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (warp_solve_structure_ok(hblk.data(), M.KV, BW1, M.ns)) {
+      if ((rc = dalloc(&s->frag, frag_doubles(M.KV, BW1, M.ns)))) return rc;
+      launch_frag_prep(s->blk, M.KV, BW1, M.ns, s->frag, st);
+    }
     CK(cudaStreamSynchronize(st));
   } else if (!rc) {
     // pass 2: columns differ -> one band and one factor per line
@@ -1270,6 +1281,7 @@ int ark_step_accumulated(atb_solver* s, double* const* q, cudaStream_t st) {
     B.M = s->M;
     B.band = s->band;
     B.blk = s->blk;
+    B.frag = s->frag;
     B.ld = s->ld;
     B.npairs = 0;
     B.dt = s->dt;
@@ -1351,6 +1363,7 @@ int ark_step(atb_solver* s, double* const* q, cudaStream_t st) {
       B.M = s->M;
       B.band = s->band;
       B.blk = s->blk;
+      B.frag = s->frag;
       B.ld = s->ld;
       B.npairs = i;
       B.dt = s->dt;

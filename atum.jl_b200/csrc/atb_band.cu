@@ -17,6 +17,8 @@
 // exists in memory.
 #include "atb_generic.cuh"
 
+#include <type_traits>
+
 namespace atb {
 
 void launch_band_solve_generic(const BandSolve& B, cudaStream_t st);
@@ -730,6 +732,326 @@ void mma_launch(const BandSolve& B, cudaStream_t st) {
   band_solve_mma_kernel<NQ, NS, NT, D><<<(B.M.nlines + LPC - 1) / LPC, NTH, smem, st>>>(B, B.blk);
 }
 
+// ---------------------------------------------- warp-owned block recurrence
+// The same recurrence (y_e = Li_e b_e - G_e y_e-1, x_e = Ui_e y_e - H_e x_e+1)
+// with one warp per 8 lines computing EVERY row of the block: the element-to-
+// element dependency stays inside the warp, so the sequential chain carries
+// no CTA barrier.  The blocks' zero structure is exploited tile by tile:
+// Li is lower and Ui upper triangular, and since DG elements couple only
+// through their face nodes, L_e,e-1 (U_e,e+1) is nonzero only in the last
+// (first) Ns columns, so G_e (H_e) is too -- the product with the previous
+// element's result needs only its face node, one or two m8n8k4 steps instead
+// of KT.  Only the nonzero 8x4 tiles are stored (frag_prep_kernel, in
+// matrix-unit fragment order: one 256-byte run per tile, one double per
+// lane), copied per element into a shared ring by the CTA with contiguous
+// 16-byte cp.async two elements ahead, and read with conflict-free 8-byte
+// loads.  The host checks the structure once (warp_solve_structure_ok) and
+// uses band_solve_mma_kernel when it does not hold.  Skipped tiles are exact
+// zeros and every accumulator adds its tiles in the same order, so the
+// results equal band_solve_mma_kernel's bit for bit.  Right-hand sides with
+// no ARK pairs only (q given whole); the other forms use band_solve_mma_kernel.
+struct TileRange {
+  int lo, hi;  // reduction steps kt = lo .. hi (inclusive) of a row tile
+};
+__host__ __device__ constexpr int imin_c(int a, int b) { return a < b ? a : b; }
+// pass 0: Li (mat 0), -G (mat 1); pass 1: Ui (mat 0), -H (mat 1); row tile mt
+__host__ __device__ constexpr TileRange tile_range(int BW1, int NS, int pass, int mat, int mt) {
+  const int KT = (BW1 + 3) / 4;
+  if (pass == 0) return mat == 0 ? TileRange{0, imin_c(KT - 1, 2 * mt + 1)} : TileRange{(BW1 - NS) / 4, KT - 1};
+  return mat == 0 ? TileRange{2 * mt, KT - 1} : TileRange{0, imin_c(KT - 1, (NS - 1) / 4)};
+}
+// tiles stored before (mat, mt) within one pass (mat-major, then mt); (2, 0) = all
+__host__ __device__ constexpr int tile_off(int BW1, int NS, int pass, int mat, int mt) {
+  const int MT = (BW1 + 7) / 8;
+  int n = 0;
+  for (int m = 0; m < 2; ++m)
+    for (int t = 0; t < MT; ++t) {
+      if (m == mat && t == mt) return n;
+      const TileRange r = tile_range(BW1, NS, pass, m, t);
+      n += r.hi - r.lo + 1;
+    }
+  return n;
+}
+__host__ __device__ constexpr int pass_tiles(int BW1, int NS, int pass) { return tile_off(BW1, NS, pass, 2, 0); }
+
+template <int BW1, int NS>
+struct WarpSolveShape {
+  static constexpr int MT = (BW1 + 7) / 8;   // row tiles
+  static constexpr int KT = (BW1 + 3) / 4;   // reduction steps
+  static constexpr int KP = 4 * KT;          // reduction length (zero rows past BW1)
+  static constexpr int RW = (KP > 8 * MT) ? KP : 8 * MT;  // rows of a result buffer
+  static constexpr int LD = 12;              // row stride of [row][line] buffers: conflict-free B fragments
+  static constexpr int T0 = pass_tiles(BW1, NS, 0), T1 = pass_tiles(BW1, NS, 1);
+  static constexpr int FR = 32 * (T0 > T1 ? T0 : T1);     // doubles of one ring slot
+  static constexpr int RS = 3;                            // ring depth (elements in flight)
+  static constexpr int WBUF = RS * KP * LD + 2 * RW * LD;  // per warp: RHS ring + 2 result buffers
+};
+
+// frag[(e * (T0 + T1) + pass * T0 + tile_off(pass, mat, mt) + kt - lo) * 32 + lane]
+//   = M[8 mt + lane / 4][4 kt + lane % 4]   (zero outside BW1 x BW1)
+// with M = Li_e, -G_e (pass 0) or Ui_e, -H_e (pass 1) for mat = 0, 1.
+__global__ void frag_prep_kernel(const double* blk, int KV, int BW1, int NS, double* frag) {
+  const int MT = (BW1 + 7) / 8;
+  const int T0 = pass_tiles(BW1, NS, 0), T1 = pass_tiles(BW1, NS, 1);
+  const size_t n = (size_t)KV * (T0 + T1) * 32;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int lane = (int)(i % 32);
+    const size_t tix = i / 32;
+    const int e = (int)(tix / (T0 + T1));
+    int t = (int)(tix - (size_t)e * (T0 + T1));
+    const int pass = t < T0 ? 0 : 1;
+    if (pass) t -= T0;
+    int mat = 0, mt = 0, kt = 0;
+    for (int m = 0; m < 2; ++m)
+      for (int r = 0; r < MT; ++r) {
+        const TileRange tr = tile_range(BW1, NS, pass, m, r);
+        const int o = tile_off(BW1, NS, pass, m, r);
+        if (t >= o && t < o + tr.hi - tr.lo + 1) {
+          mat = m;
+          mt = r;
+          kt = tr.lo + t - o;
+        }
+      }
+    const int row = 8 * mt + lane / 4, col = 4 * kt + lane % 4;
+    double v = 0.0;
+    if (row < BW1 && col < BW1) {
+      const double* m = blk + ((size_t)e * 4 + 2 * pass + mat) * BW1 * BW1;
+      v = m[row * BW1 + col];
+      if (mat == 1) v = -v;
+    }
+    frag[i] = v;
+  }
+}
+
+__device__ __forceinline__ void cp_async16g(void* smem, const void* gmem) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+template <int NQ, int NS, int NW>
+__global__ void __launch_bounds__(32 * NW) band_solve_warp_kernel(const BandSolve B) {
+  constexpr int BW1 = NQ * NS;
+  using S = WarpSolveShape<BW1, NS>;
+  constexpr int MT = S::MT, KT = S::KT, KP = S::KP, RW = S::RW, LD = S::LD, FR = S::FR, RS = S::RS;
+  constexpr int T0 = S::T0, T1 = S::T1;
+  constexpr int JT = (BW1 + 3) / 4;  // RHS rows per lane per element (4 rows x 8 lines per pass)
+  extern __shared__ __align__(16) double sm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, tq = lane & 3;
+  double* Fr = sm;                                   // [RS][FR], shared by the CTA's warps
+  double* ring = sm + RS * FR + warp * S::WBUF;      // [RS][KP][LD]: right-hand sides
+  double* Wb = ring + RS * KP * LD;                  // [2][RW][LD]: results of the last two elements
+  const LineMap& M = B.M;
+  const int KV = M.KV, nh = M.nh, Np = M.Np;
+  const size_t lstep = (size_t)M.estep * Np;
+  const int line0 = (blockIdx.x * NW + warp) * 8;
+  for (int i = lane; i < S::WBUF; i += 32) ring[i] = 0.0;
+  // ---- RHS loader: lane owns line (lane & 7) and rows 4j + (lane >> 3)
+  const int ll = lane & 7;
+  const bool lact = line0 + ll < M.nlines;
+  const size_t lb = lact ? (size_t)M.e0[line0 + ll] * Np + (line0 + ll) % nh : 0;
+  size_t roff[JT];
+  int rsel[JT];
+#pragma unroll
+  for (int j = 0; j < JT; ++j) {
+    const int row = 4 * j + (lane >> 3);
+    rsel[j] = (lact && row < BW1) ? row % NS : -1;
+    roff[j] = lb + (row < BW1 ? (size_t)nh * (row / NS) : 0);
+  }
+  auto field = [&](auto f, int s) {
+    auto p = f[0];
+#pragma unroll
+    for (int c = 1; c < NS; ++c)
+      if (c == s) p = f[c];
+    return p;
+  };
+  const double* src[JT];
+#pragma unroll
+  for (int j = 0; j < JT; ++j) src[j] = field(B.q, rsel[j] < 0 ? 0 : rsel[j]) + roff[j];
+  // ---- outputs: rows 8 mt + g, lines 2 tq + i
+  double* dst[MT];
+#pragma unroll
+  for (int mt = 0; mt < MT; ++mt) {
+    const int row = 8 * mt + g;
+    dst[mt] = field(B.out, row < BW1 ? row % NS : 0) + (row < BW1 ? (size_t)nh * (row / NS) : 0);
+  }
+  size_t obase[2];
+  bool oact[2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const int line = line0 + 2 * tq + i;
+    oact[i] = line < M.nlines;
+    obase[i] = oact[i] ? (size_t)M.e0[line] * Np + line % nh : 0;
+  }
+  // element ev of pass p (its tiles and this warp's RHS) into ring slot ev % RS
+  auto issue = [&](int ev, int pass) {
+    if (ev >= 0 && ev < KV) {
+      const int slot = ev % RS;
+      const double* gf = B.frag + ((size_t)ev * (T0 + T1) + (pass ? T0 : 0)) * 32;
+      double* sf = Fr + slot * FR;
+      const int n16 = (pass ? T1 : T0) * 16;
+      for (int c = threadIdx.x; c < n16; c += 32 * NW) cp_async16g(sf + 2 * c, gf + 2 * c);
+      double* sr = ring + slot * KP * LD;
+#pragma unroll
+      for (int j = 0; j < JT; ++j)
+        if (rsel[j] >= 0) cp_async8(sr + (4 * j + (lane >> 3)) * LD + ll, src[j] + (size_t)ev * lstep);
+    }
+    cp_async_commit();
+  };
+  auto step = [&](auto passc, int ev, int par) {
+    constexpr int P = decltype(passc)::value;
+    const double* F = Fr + (ev % RS) * FR + lane;
+    const double* V = ring + (ev % RS) * KP * LD;
+    const double* Wp = Wb + (par ^ 1) * RW * LD;
+    double* Wn = Wb + par * RW * LD;
+    constexpr TileRange cr = tile_range(BW1, NS, P, 1, 0);  // the same for every row tile
+    double bv[KT], bw[KT];
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt) {
+      bv[kt] = V[(4 * kt + tq) * LD + g];
+      bw[kt] = (kt >= cr.lo && kt <= cr.hi) ? Wp[(4 * kt + tq) * LD + g] : 0.0;
+    }
+    double aA[MT][2], aC[MT][2];
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) {
+      aA[mt][0] = aA[mt][1] = aC[mt][0] = aC[mt][1] = 0.0;
+    }
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) {
+      const TileRange ra = tile_range(BW1, NS, P, 0, mt);
+      const int oa = tile_off(BW1, NS, P, 0, mt), oc = tile_off(BW1, NS, P, 1, mt);
+#pragma unroll
+      for (int kt = 0; kt < KT; ++kt) {
+        if (kt >= ra.lo && kt <= ra.hi) dmma_8x8x4(aA[mt][0], aA[mt][1], F[(oa + kt - ra.lo) * 32], bv[kt]);
+        if (kt >= cr.lo && kt <= cr.hi) dmma_8x8x4(aC[mt][0], aC[mt][1], F[(oc + kt - cr.lo) * 32], bw[kt]);
+      }
+    }
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) {
+      const int row = 8 * mt + g;
+      const double y0 = aA[mt][0] + aC[mt][0], y1 = aA[mt][1] + aC[mt][1];
+      *reinterpret_cast<double2*>(Wn + row * LD + 2 * tq) = make_double2(y0, y1);
+      if (row < BW1) {
+        if (oact[0]) dst[mt][obase[0] + (size_t)ev * lstep] = y0;
+        if (oact[1]) dst[mt][obase[1] + (size_t)ev * lstep] = y1;
+      }
+    }
+  };
+  __syncthreads();
+  // ------------------------------------------------------------ forward
+  issue(0, 0);
+  issue(1, 0);
+  for (int ev = 0; ev < KV; ++ev) {
+    cp_async_wait<1>();
+    __syncthreads();  // element ev in place; every warp is past element ev-1
+    issue(ev + 2, 0);
+    step(std::integral_constant<int, 0>{}, ev, ev & 1);
+  }
+  cp_async_wait<0>();
+  __syncthreads();  // the forward results are written (the backward pass reads them)
+  // ----------------------------------------------------------- backward
+#pragma unroll
+  for (int j = 0; j < JT; ++j) src[j] = field(B.out, rsel[j] < 0 ? 0 : rsel[j]) + roff[j];
+  // x_KV = 0: the buffer read first holds zeros
+  for (int i = lane; i < RW * LD; i += 32) Wb[((KV & 1) ^ 1) * RW * LD + i] = 0.0;
+  issue(KV - 1, 1);
+  issue(KV - 2, 1);
+  for (int t = 0; t < KV; ++t) {
+    const int ev = KV - 1 - t;
+    cp_async_wait<1>();
+    __syncthreads();
+    issue(ev - 2, 1);
+    step(std::integral_constant<int, 1>{}, ev, (KV + t) & 1);
+  }
+  cp_async_wait<0>();
+}
+
+template <int NQ, int NS, int NW>
+constexpr size_t warp_solve_smem() {
+  using S = WarpSolveShape<NQ * NS, NS>;
+  return sizeof(double) * ((size_t)S::RS * S::FR + (size_t)NW * S::WBUF);
+}
+
+constexpr size_t kWarpSolveSmemMax = 227 * 1024;
+
+template <int NQ, int NS, int NW>
+void warp_launch_nw(const BandSolve& B, cudaStream_t st) {
+  constexpr size_t smem = warp_solve_smem<NQ, NS, NW>();
+  static bool configured = false;
+  if (!configured && smem > 48 * 1024)
+    cudaFuncSetAttribute(band_solve_warp_kernel<NQ, NS, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  configured = true;
+  const int warps = (B.M.nlines + 7) / 8;
+  band_solve_warp_kernel<NQ, NS, NW><<<(warps + NW - 1) / NW, 32 * NW, smem, st>>>(B);
+}
+
+// Warps per CTA: the element steps are bound by the issue rate of each SM, so
+// the time goes with the warps the busiest SM runs in total, ceil(CTAs / SMs)
+// x NW; among counts within 2% of each other, CTAs on every SM, then more
+// warps resident at once (latency hiding), then more warps per CTA (each copy
+// of the tiles shared by more lines).
+inline int pick_nw(int warps, int nsm, const size_t smem[4]) {
+  static const int cand[4] = {2, 3, 4, 6};
+  int best = -1;
+  long best_load = 0;
+  int best_sms = 0, best_res = 0;
+  for (int i = 0; i < 4; ++i) {
+    if (smem[i] > kWarpSolveSmemMax) continue;
+    const int nw = cand[i];
+    const long ctas = (warps + nw - 1) / nw;
+    int cps = (int)((228 * 1024) / (smem[i] + 1024));
+    if (cps > 2048 / (32 * nw)) cps = 2048 / (32 * nw);
+    if (cps < 1) continue;
+    const long per_sm = (ctas + nsm - 1) / nsm;
+    const long load = per_sm * nw;
+    const int sms = (int)(ctas < nsm ? ctas : nsm);
+    const int res = (int)((per_sm < cps ? per_sm : cps) * nw);
+    const bool better = best < 0 || 50 * load < 49 * best_load;
+    const bool close = best >= 0 && 50 * load <= 51 * best_load && 50 * best_load <= 51 * load;
+    if (better || (close && (sms > best_sms || (sms == best_sms && res >= best_res)))) {
+      best = nw;
+      best_load = load;
+      best_sms = sms;
+      best_res = res;
+    }
+  }
+  return best;
+}
+
+template <int NQ, int NS>
+bool warp_launch(const BandSolve& B, cudaStream_t st) {
+  static int nsm = 0;
+  if (!nsm) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (nsm <= 0) nsm = 148;
+  }
+  const size_t smem[4] = {warp_solve_smem<NQ, NS, 2>(), warp_solve_smem<NQ, NS, 3>(), warp_solve_smem<NQ, NS, 4>(),
+                          warp_solve_smem<NQ, NS, 6>()};
+  switch (pick_nw((B.M.nlines + 7) / 8, nsm, smem)) {
+    case 2: warp_launch_nw<NQ, NS, 2>(B, st); return true;
+    case 3: warp_launch_nw<NQ, NS, 3>(B, st); return true;
+    case 4: warp_launch_nw<NQ, NS, 4>(B, st); return true;
+    case 6: warp_launch_nw<NQ, NS, 6>(B, st); return true;
+  }
+  return false;
+}
+
+typedef bool (*warp_fn)(const BandSolve&, cudaStream_t);
+template <int NS> warp_fn pick_warp(int nq) {
+  switch (nq) {
+    case 2: return warp_launch<2, NS>;
+    case 3: return warp_launch<3, NS>;
+    case 4: return warp_launch<4, NS>;
+    case 5: return warp_launch<5, NS>;
+    case 6: return warp_launch<6, NS>;
+    case 7: return warp_launch<7, NS>;
+    case 8: return warp_launch<8, NS>;
+  }
+  return nullptr;
+}
+
 template <int NS> solve_fn pick_mma(int nq) {
   switch (nq) {
     case 2: return mma_launch<2, NS>;
@@ -762,11 +1084,42 @@ void launch_block_prep(const double* band, int KV, int BW1, double* blk, cudaStr
   block_prep_kernel<<<KV, ((BW1 + 31) / 32) * 32, 0, st>>>(band, KV, BW1, blk);
 }
 
+size_t frag_doubles(int KV, int BW1, int NS) {
+  return (size_t)KV * (pass_tiles(BW1, NS, 0) + pass_tiles(BW1, NS, 1)) * 32;
+}
+
+void launch_frag_prep(const double* blk, int KV, int BW1, int NS, double* frag, cudaStream_t st) {
+  const size_t n = frag_doubles(KV, BW1, NS);
+  const int blocks = (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
+  frag_prep_kernel<<<blocks, 256, 0, st>>>(blk, KV, BW1, NS, frag);
+}
+
+bool warp_solve_structure_ok(const double* blk_host, int KV, int BW1, int NS) {
+  // every nonzero of Li, G, Ui, H lies inside the stored tiles of its row tile
+  const int MT = (BW1 + 7) / 8;
+  for (int e = 0; e < KV; ++e)
+    for (int pass = 0; pass < 2; ++pass)
+      for (int mat = 0; mat < 2; ++mat) {
+        const double* m = blk_host + ((size_t)e * 4 + 2 * pass + mat) * BW1 * BW1;
+        for (int mt = 0; mt < MT; ++mt) {
+          const TileRange r = tile_range(BW1, NS, pass, mat, mt);
+          for (int row = 8 * mt; row < 8 * mt + 8 && row < BW1; ++row)
+            for (int col = 0; col < BW1; ++col)
+              if ((col < 4 * r.lo || col > 4 * r.hi + 3) && m[row * BW1 + col] != 0.0) return false;
+        }
+      }
+  return true;
+}
+
 
 // Dispatch: the block-parallel form when the factor is shared and its
 // per-element inverses were prepared, else the register-window substitution
 // (shared factor), else the generic per-line kernel.
 void launch_band_solve(const BandSolve& B, cudaStream_t st) {
+  if (B.ld == 1 && B.frag && B.npairs == 0 && (B.M.ns == 4 || B.M.ns == 5)) {
+    warp_fn w = B.M.ns == 4 ? pick_warp<4>(B.M.Nq) : pick_warp<5>(B.M.Nq);
+    if (w && w(B, st)) return;
+  }
   solve_fn f = nullptr;
   if (B.ld == 1 && B.blk) {
     if (B.M.ns == 1) f = pick_rows<1>(B.M.Nq);

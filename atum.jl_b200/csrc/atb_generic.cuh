@@ -70,9 +70,15 @@ struct BandSolve {
   const double* im[2][5];
   double* out[5];
   const double* blk;  // per-element [L^-1 | G | U^-1 | H] blocks (shared factor), or null
+  const double* frag; // the same blocks in matrix-unit fragment order (launch_frag_prep), or null
 };
 void launch_band_solve(const BandSolve& B, cudaStream_t st);
 void launch_block_prep(const double* band, int KV, int BW1, double* blk, cudaStream_t st);
+// the per-element tiles of the warp-owned solve (band_solve_warp_kernel)
+size_t frag_doubles(int KV, int BW1, int NS);
+void launch_frag_prep(const double* blk, int KV, int BW1, int NS, double* frag, cudaStream_t st);
+// whether the blocks (host copy of blk) have the zero structure those tiles assume
+bool warp_solve_structure_ok(const double* blk_host, int KV, int BW1, int NS);
 
 void launch_red_finish(const double* partials, int nblocks, int linf, double* out5, cudaStream_t st);
 double probe_fp64_tflops(cudaStream_t st);
