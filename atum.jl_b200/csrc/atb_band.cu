@@ -868,40 +868,41 @@ __global__ void __launch_bounds__(32 * NW) band_solve_warp_kernel(const BandSolv
   const double* src[JT];
 #pragma unroll
   for (int j = 0; j < JT; ++j) src[j] = field(B.q, rsel[j] < 0 ? 0 : rsel[j]) + roff[j];
-  // ---- outputs: rows 8 mt + g, lines 2 tq + i
-  double* dst[MT];
-#pragma unroll
-  for (int mt = 0; mt < MT; ++mt) {
-    const int row = 8 * mt + g;
-    dst[mt] = field(B.out, row < BW1 ? row % NS : 0) + (row < BW1 ? (size_t)nh * (row / NS) : 0);
-  }
-  size_t obase[2];
-  bool oact[2];
+  // ---- outputs: rows 8 mt + g, lines 2 tq + i (null: padding row or no line)
+  double* dst[MT][2];
 #pragma unroll
   for (int i = 0; i < 2; ++i) {
     const int line = line0 + 2 * tq + i;
-    oact[i] = line < M.nlines;
-    obase[i] = oact[i] ? (size_t)M.e0[line] * Np + line % nh : 0;
+    const bool act = line < M.nlines;
+    const size_t ob = act ? (size_t)M.e0[line] * Np + line % nh : 0;
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) {
+      const int row = 8 * mt + g;
+      dst[mt][i] = (act && row < BW1) ? field(B.out, row % NS) + (size_t)nh * (row / NS) + ob : nullptr;
+    }
   }
-  // element ev of pass p (its tiles and this warp's RHS) into ring slot ev % RS
-  auto issue = [&](int ev, int pass) {
+  // element ev of pass P (its tiles and this warp's RHS) into ring slot
+  // ev % RS; evoff = ev * (element step in the fields)
+  auto issue = [&](auto passc, int ev, int slot, size_t evoff) {
+    constexpr int P = decltype(passc)::value;
     if (ev >= 0 && ev < KV) {
-      const int slot = ev % RS;
-      const double* gf = B.frag + ((size_t)ev * (T0 + T1) + (pass ? T0 : 0)) * 32;
-      double* sf = Fr + slot * FR;
-      const int n16 = (pass ? T1 : T0) * 16;
-      for (int c = threadIdx.x; c < n16; c += 32 * NW) cp_async16g(sf + 2 * c, gf + 2 * c);
-      double* sr = ring + slot * KP * LD;
+      constexpr int n16 = (P ? T1 : T0) * 16;
+      const double* gf = B.frag + ((size_t)ev * (T0 + T1) + (P ? T0 : 0)) * 32 + 2 * threadIdx.x;
+      double* sf = Fr + slot * FR + 2 * threadIdx.x;
+#pragma unroll
+      for (int c = 0; c < n16; c += 32 * NW)
+        if (c + (int)threadIdx.x < n16) cp_async16g(sf + 2 * c, gf + 2 * c);
+      double* sr = ring + slot * KP * LD + (lane >> 3) * LD + ll;
 #pragma unroll
       for (int j = 0; j < JT; ++j)
-        if (rsel[j] >= 0) cp_async8(sr + (4 * j + (lane >> 3)) * LD + ll, src[j] + (size_t)ev * lstep);
+        if (rsel[j] >= 0) cp_async8(sr + 4 * j * LD, src[j] + evoff);
     }
     cp_async_commit();
   };
-  auto step = [&](auto passc, int ev, int par) {
+  auto step = [&](auto passc, int slot, size_t evoff, int par) {
     constexpr int P = decltype(passc)::value;
-    const double* F = Fr + (ev % RS) * FR + lane;
-    const double* V = ring + (ev % RS) * KP * LD;
+    const double* F = Fr + slot * FR + lane;
+    const double* V = ring + slot * KP * LD;
     const double* Wp = Wb + (par ^ 1) * RW * LD;
     double* Wn = Wb + par * RW * LD;
     constexpr TileRange cr = tile_range(BW1, NS, P, 1, 0);  // the same for every row tile
@@ -931,21 +932,30 @@ __global__ void __launch_bounds__(32 * NW) band_solve_warp_kernel(const BandSolv
       const int row = 8 * mt + g;
       const double y0 = aA[mt][0] + aC[mt][0], y1 = aA[mt][1] + aC[mt][1];
       *reinterpret_cast<double2*>(Wn + row * LD + 2 * tq) = make_double2(y0, y1);
-      if (row < BW1) {
-        if (oact[0]) dst[mt][obase[0] + (size_t)ev * lstep] = y0;
-        if (oact[1]) dst[mt][obase[1] + (size_t)ev * lstep] = y1;
-      }
+      if (dst[mt][0]) dst[mt][0][evoff] = y0;
+      if (dst[mt][1]) dst[mt][1][evoff] = y1;
     }
   };
+  const std::integral_constant<int, 0> fwd{};
+  const std::integral_constant<int, 1> bwd{};
   __syncthreads();
   // ------------------------------------------------------------ forward
-  issue(0, 0);
-  issue(1, 0);
-  for (int ev = 0; ev < KV; ++ev) {
-    cp_async_wait<1>();
-    __syncthreads();  // element ev in place; every warp is past element ev-1
-    issue(ev + 2, 0);
-    step(std::integral_constant<int, 0>{}, ev, ev & 1);
+  // slot: ev % RS; the refill of slot (ev + 2) % RS = (ev - 1) % RS follows
+  // the barrier that ends every warp's use of it and this warp's step ev
+  issue(fwd, 0, 0, 0);
+  issue(fwd, 1, 1, lstep);
+  {
+    int slot = 0;
+    size_t evoff = 0;
+    for (int ev = 0; ev < KV; ++ev) {
+      cp_async_wait<1>();
+      __syncthreads();  // element ev in place; every warp is past element ev-1
+      step(fwd, slot, evoff, ev & 1);
+      const int s2 = slot == 0 ? RS - 1 : slot - 1;
+      issue(fwd, ev + 2, s2, evoff + 2 * lstep);
+      slot = slot == RS - 1 ? 0 : slot + 1;
+      evoff += lstep;
+    }
   }
   cp_async_wait<0>();
   __syncthreads();  // the forward results are written (the backward pass reads them)
@@ -954,14 +964,22 @@ __global__ void __launch_bounds__(32 * NW) band_solve_warp_kernel(const BandSolv
   for (int j = 0; j < JT; ++j) src[j] = field(B.out, rsel[j] < 0 ? 0 : rsel[j]) + roff[j];
   // x_KV = 0: the buffer read first holds zeros
   for (int i = lane; i < RW * LD; i += 32) Wb[((KV & 1) ^ 1) * RW * LD + i] = 0.0;
-  issue(KV - 1, 1);
-  issue(KV - 2, 1);
-  for (int t = 0; t < KV; ++t) {
-    const int ev = KV - 1 - t;
-    cp_async_wait<1>();
-    __syncthreads();
-    issue(ev - 2, 1);
-    step(std::integral_constant<int, 1>{}, ev, (KV + t) & 1);
+  // slot: (KV - 1 - ev) % RS, i.e. the step count t % RS
+  issue(bwd, KV - 1, 0, (size_t)(KV - 1) * lstep);
+  issue(bwd, KV - 2, 1, (size_t)(KV - 2) * lstep);
+  {
+    int slot = 0;
+    size_t evoff = (size_t)(KV - 1) * lstep;
+    for (int t = 0; t < KV; ++t) {
+      const int ev = KV - 1 - t;
+      cp_async_wait<1>();
+      __syncthreads();
+      step(bwd, slot, evoff, (KV + t) & 1);
+      const int s2 = slot == 0 ? RS - 1 : slot - 1;
+      issue(bwd, ev - 2, s2, evoff - 2 * lstep);
+      slot = slot == RS - 1 ? 0 : slot + 1;
+      evoff -= lstep;
+    }
   }
   cp_async_wait<0>();
 }
