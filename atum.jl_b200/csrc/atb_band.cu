@@ -18,6 +18,7 @@
 #include "atb_generic.cuh"
 
 #include <type_traits>
+#include <utility>
 
 namespace atb {
 
@@ -823,6 +824,17 @@ __global__ void frag_prep_kernel(const double* blk, int KV, int BW1, int NS, dou
   }
 }
 
+// f(integral_constant<int, 0>) ... f(integral_constant<int, N-1>): loop
+// indices that are constant expressions inside the body
+template <class Fn, int... I>
+__device__ __forceinline__ void static_for_impl(Fn& f, std::integer_sequence<int, I...>) {
+  (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, class Fn>
+__device__ __forceinline__ void static_for(Fn&& f) {
+  static_for_impl(f, std::make_integer_sequence<int, N>{});
+}
+
 __device__ __forceinline__ void cp_async16g(void* smem, const void* gmem) {
   unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
@@ -917,16 +929,33 @@ __global__ void __launch_bounds__(32 * NW) band_solve_warp_kernel(const BandSolv
     for (int mt = 0; mt < MT; ++mt) {
       aA[mt][0] = aA[mt][1] = aC[mt][0] = aC[mt][1] = 0.0;
     }
-#pragma unroll
-    for (int mt = 0; mt < MT; ++mt) {
-      const TileRange ra = tile_range(BW1, NS, P, 0, mt);
-      const int oa = tile_off(BW1, NS, P, 0, mt), oc = tile_off(BW1, NS, P, 1, mt);
-#pragma unroll
-      for (int kt = 0; kt < KT; ++kt) {
-        if (kt >= ra.lo && kt <= ra.hi) dmma_8x8x4(aA[mt][0], aA[mt][1], F[(oa + kt - ra.lo) * 32], bv[kt]);
-        if (kt >= cr.lo && kt <= cr.hi) dmma_8x8x4(aC[mt][0], aC[mt][1], F[(oc + kt - cr.lo) * 32], bw[kt]);
-      }
-    }
+    // reduction step outermost: consecutive matrix-unit operations feed
+    // different accumulators (a dependent one waits the full latency); each
+    // accumulator still adds its tiles in ascending kt.  The coupling
+    // product (previous element) first: its operands are the ones produced
+    // last.  Tile offsets are constant expressions (static_for indices).
+    static_for<KT>([&](auto ktc) {
+      constexpr int kt = decltype(ktc)::value;
+      static_for<MT>([&](auto mtc) {
+        constexpr int mt = decltype(mtc)::value;
+        constexpr TileRange rc = tile_range(BW1, NS, P, 1, mt);
+        if constexpr (kt >= rc.lo && kt <= rc.hi) {
+          constexpr int off = (tile_off(BW1, NS, P, 1, mt) + kt - rc.lo) * 32;
+          dmma_8x8x4(aC[mt][0], aC[mt][1], F[off], bw[kt]);
+        }
+      });
+    });
+    static_for<KT>([&](auto ktc) {
+      constexpr int kt = decltype(ktc)::value;
+      static_for<MT>([&](auto mtc) {
+        constexpr int mt = decltype(mtc)::value;
+        constexpr TileRange ra = tile_range(BW1, NS, P, 0, mt);
+        if constexpr (kt >= ra.lo && kt <= ra.hi) {
+          constexpr int off = (tile_off(BW1, NS, P, 0, mt) + kt - ra.lo) * 32;
+          dmma_8x8x4(aA[mt][0], aA[mt][1], F[off], bv[kt]);
+        }
+      });
+    });
 #pragma unroll
     for (int mt = 0; mt < MT; ++mt) {
       const int row = 8 * mt + g;
