@@ -292,8 +292,14 @@ def run_ours(args):
     case = build_case(args.precision, scheme=scheme)
     dofs = case.q0.size
     q = torch.as_tensor(case.q0, device="cuda").contiguous()
-    # launch shapes picked by the library's autotuner (results do not depend on them)
-    tuned = {"tendency": A.batch.autotune(case.dg, q)}
+    # launch shapes picked by the library's autotuner (results do not depend on
+    # them), or the explicit operator's given (a profiler's replays perturb the
+    # autotuner's timings)
+    if args.elements_per_cta:
+        A.batch.set_launch(case.dg, args.elements_per_cta)
+        tuned = {"tendency": args.elements_per_cta}
+    else:
+        tuned = {"tendency": A.batch.autotune(case.dg, q)}
     if scheme == "ark23":
         tuned["tendency_linear"] = A.batch.autotune(case.lindg, q)
     solver = make_solver(A, case, q, scheme)
@@ -878,6 +884,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32flux"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--elements-per-cta", type=int, default=0,
+                    help="bubble: launch shape of the explicit operator (elements per CTA) instead of autotuning")
     ap.add_argument("--scheme", default="ark23", choices=sorted(SCHEME_STAGES),
                     help="time stepper of the bubble workload: IMEX ARK23 (default) or the fully explicit LSRK54 "
                          "run of the same problem")
