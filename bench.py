@@ -699,7 +699,7 @@ def run_c5(args):
             avgb = b["ms"] / b["launches"]
             # right-hand side read, solution written, read back and rewritten
             byt = 4 * dofs * 8
-            out["band_solve"] = {"kernel": "band_solve_mma_kernel<8,5>", "avg_launch_ms": avgb, "bound": "hbm",
+            out["band_solve"] = {"kernel": "band_solve_warp_kernel<8,5> (tile-sparse warp-owned recurrence)", "avg_launch_ms": avgb, "bound": "hbm",
                                  "achieved_gbs": byt / (avgb * 1e-3) / 1e9, "peak_gbs": peaks["hbm_gbs"],
                                  "frac": byt / (avgb * 1e-3) / 1e9 / peaks["hbm_gbs"], "peak_kind": kind}
         out["launch_totals"] = prof
