@@ -560,6 +560,10 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
     if constexpr (PAIRS) {
       // ---- phase A: each unordered pair of each line of direction d once
       if (act) {
+        // two pairs per thread per direction at N=4: unrolled, the fused ARK
+        // kernel interleaves their flux chains (measured 3% faster); the
+        // plain kernel is faster rolled
+#pragma unroll(FUSE ? 2 : 1)
         for (int t = node; t < Nfp * npl; t += Np) {
           const int line = t / npl, p = t - line * npl;
           const int lb = (d == 0) ? line * Nq : (d == 1) ? (line % Nq) + Nq * Nq * (line / Nq) : line;
