@@ -69,6 +69,7 @@ SIGNATURES = {
     "atb_solve": [_VP, PtrArr, C.c_double, C.c_int, _IP, _VP],
     "atb_solver_get": [_VP, _DP, _DP, _DP],
     "atb_solver_set_dt": [_VP, C.c_double],
+    "atb_solver_set_state": [_VP, C.c_double, C.c_double],
     "atb_solver_set_instance_dt": [_VP, _DP],
     "atb_solver_set_element_dt": [_VP, _DP],
     "atb_solver_fuse": [_VP, C.c_int],

@@ -1542,6 +1542,14 @@ extern "C" int atb_solver_get(const atb_solver* s, double* time, double* dt, dou
   return ATB_OK;
 }
 
+extern "C" int atb_solver_set_state(atb_solver* s, double time, double gamma) {
+  if (!s) return fail(ATB_ERR_INVALID, "null solver");
+  if (!std::isfinite(time) || !std::isfinite(gamma)) return fail(ATB_ERR_INVALID, "non-finite solver state");
+  s->time = time;
+  s->gamma_r = gamma;
+  return ATB_OK;
+}
+
 extern "C" int atb_solver_set_dt(atb_solver* s, double dt) {
   if (!s) return fail(ATB_ERR_INVALID, "null solver");
   if (s->kind == ATB_ARK23 && s->lin && dt != s->dt)

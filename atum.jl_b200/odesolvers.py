@@ -64,6 +64,15 @@ class Solver:
     def gamma(self) -> float:
         return self._get()[2]
 
+    def state(self) -> dict:
+        """The solver scalars a checkpoint needs (``atum_b200.checkpoint``)."""
+        t, dt, g = self._get()
+        return {"kind": self.kind, "time": t, "dt": dt, "gamma": g}
+
+    def set_state(self, time: float, gamma: float = 1.0):
+        """Restores the clock and the last relaxation factor of a checkpoint."""
+        _lib.check(_lib.lib().atb_solver_set_state(self.h, float(time), float(gamma)))
+
     def fuse(self, enable: bool = True):
         """ARK23: run the explicit and the linear operator of a stage as one
         kernel (on by default when the operators allow it)."""

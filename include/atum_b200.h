@@ -183,6 +183,13 @@ int atb_solver_step(atb_solver* s, double* const* q, int nsteps, void* stream);
 int atb_solve(atb_solver* s, double* const* q, double timeend, int adjust_final, int* steps_out, void* stream);
 int atb_solver_get(const atb_solver* s, double* time, double* dt, double* gamma);
 int atb_solver_set_dt(atb_solver* s, double dt);
+/* Checkpoint / resume (no reference counterpart: the reference writes only VTK
+ * snapshots, experiment/euler_gravity/risingbubble.jl:81-95): restores the
+ * clock and the last relaxation factor (the RLSRK Newton's starting point)
+ * that atb_solver_get reported, so a solver rebuilt on the same operators and
+ * dt continues a checkpointed run bit for bit.  Non-finite values are
+ * rejected. */
+int atb_solver_set_state(atb_solver* s, double time, double gamma);
 /* Per-instance time steps for an LSRK solver over a packed operator (no
  * reference counterpart): dt_host holds one step per instance (host memory,
  * copied synchronously; 0 freezes an instance); NULL returns to the solver's
