@@ -4,16 +4,17 @@ The reference has no checkpoint (its experiments write VTK snapshots only,
 experiment/euler_gravity/risingbubble.jl:81-95); this is the raw form a run
 needs to stop and continue: the ``Ns`` state components exactly as they sit in
 device memory (float64, one contiguous ``K*Np`` array per component, node
-fastest) and the solver's clock, time step and last relaxation factor.  A
-solver rebuilt on the same operators and time step, given the state back with
-``resume``, continues the run bit for bit.
+fastest; the array's own shape, components first, is kept) and the solver's
+clock, time step and last relaxation factor.  A solver rebuilt on the same
+operators and time step, given the state back with ``resume``, continues the
+run bit for bit.
 
 File layout (little-endian)::
 
     8 bytes   b"ATBCKPT1"
     8 bytes   uint64 header length H
-    H bytes   JSON header: {"ns", "n", "dtype": "float64", "solver": {...} | null,
-                            "meta": {...}}
+    H bytes   JSON header: {"shape": [Ns, ...], "ns", "n", "dtype": "float64",
+                            "solver": {...} | null, "meta": {...}}
     ns*n*8    the components, one after another
 
 ``save`` copies a device state to the host (one synchronous copy per call);
@@ -40,8 +41,8 @@ def _host_array(q) -> np.ndarray:
     a = np.asarray(a)
     if a.dtype != np.float64:
         raise TypeError(f"checkpoint states are float64 (got {a.dtype})")
-    if a.ndim != 2:
-        raise ValueError(f"expected an (Ns, K*Np) state, got shape {a.shape}")
+    if a.ndim < 2:
+        raise ValueError(f"expected a state with its components first, got shape {a.shape}")
     return np.ascontiguousarray(a)
 
 
@@ -50,7 +51,8 @@ def save(path: str, q, solver=None, meta: dict | None = None) -> dict:
     is written to a temporary name first and renamed, so a reader never sees a
     partial checkpoint.  Returns the header."""
     a = _host_array(q)
-    header = {"ns": int(a.shape[0]), "n": int(a.shape[1]), "dtype": "float64",
+    header = {"shape": [int(d) for d in a.shape], "ns": int(a.shape[0]), "n": int(a.size // a.shape[0]),
+              "dtype": "float64",
               "solver": solver.state() if solver is not None else None, "meta": meta or {}}
     hb = json.dumps(header, sort_keys=True).encode()
     tmp = path + ".tmp"
@@ -78,7 +80,8 @@ def load(path: str, device=None):
         raw = f.read(ns * n * 8)
         if len(raw) != ns * n * 8:
             raise ValueError(f"{path}: truncated ({len(raw)} of {ns * n * 8} state bytes)")
-    q = np.frombuffer(raw, dtype="<f8").reshape(ns, n).astype(np.float64, copy=True)
+    shape = tuple(header.get("shape") or (ns, n))
+    q = np.frombuffer(raw, dtype="<f8").reshape(shape).astype(np.float64, copy=True)
     if device is not None:
         import torch
         q = torch.as_tensor(q, device=device).contiguous()

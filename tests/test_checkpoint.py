@@ -25,9 +25,9 @@ class _FakeSolver:
 
 def test_format_round_trip(tmp_path):
     rng = np.random.default_rng(7)
-    q = rng.standard_normal((5, 1000))
-    q[2, 3] = -0.0
-    q[4, 7] = 1e-310  # subnormal
+    q = rng.standard_normal((5, 40, 25))  # (Ns, K, Np), as the state arrays are
+    q[2, 3, 0] = -0.0
+    q[4, 7, 1] = 1e-310  # subnormal
     p = str(tmp_path / "run.ckpt")
     h = CK.save(p, q, _FakeSolver(), meta={"step": 40})
     q2, h2 = CK.load(p)
@@ -50,6 +50,8 @@ def test_damaged_files_rejected(tmp_path):
         CK.load(p)
     with pytest.raises(TypeError):
         CK.save(p, q.astype(np.float32))
+    with pytest.raises(ValueError, match="components first"):
+        CK.save(p, np.zeros(10))
     with pytest.raises(ValueError, match="no solver state"):
         CK.resume(_FakeSolver(), {"solver": None})
 
