@@ -1,20 +1,29 @@
 // Batched vertical banded solve for the IMEX implicit stage (the solve of
-// I - dt a_ii L_vert, src/odesolvers.jl:351-356), fast path for a factor
+// I - dt a_ii L_vert, src/odesolvers.jl:351-356), fast paths for a factor
 // shared by every vertical column.
 //
 // Structure: the unknowns of a vertical line, ordered (element, node, state),
 // give a band of half-width bw = Nq*ns - 1 = BW1 - 1, so row i of element ev
 // couples only to the BW1 unknowns of elements ev-1, ev (forward) or ev, ev+1
-// (backward).  One thread owns one line; its window of solution values is two
-// register arrays (previous / current element) with every index known at
-// compile time, so the inner products are fully unrolled FMAs with no local
-// memory.  The factor block of one element (BW1 rows x 2*BW1 padded columns,
-// 16*BW1^2 bytes) is the same for all lines of the CTA: it is staged into
-// shared memory with cp.async, double-buffered so the copy of element ev+1
-// overlaps the arithmetic of element ev, and read back as warp broadcasts.
-// The ARK right-hand side q + dt sum_k (a_k ex_k + b_k im_k) is formed on the
-// fly as each row is reached (src/odesolvers.jl:346-349), so Qhat never
-// exists in memory.
+// (backward).  The ARK right-hand side q + dt sum_k (a_k ex_k + b_k im_k) is
+// formed on the fly as each row is reached (src/odesolvers.jl:346-349), so
+// Qhat never exists in memory.  Kernels, in the order launch_band_solve
+// prefers them:
+//   band_solve_warp_kernel   block recurrence on the FP64 matrix unit, one
+//                            warp per 8 lines, nonzero tiles only (ARK stages
+//                            whose right-hand side is given whole)
+//   band_solve_mma_kernel    the same over dense blocks, one warp per 8 rows
+//   band_solve_rows_kernel   one-state laws
+//   band_solve_shared_kernel substitution over the shared factor (below)
+// and launch_band_solve_generic (atb_generic.cu) for a factor per line.
+//
+// band_solve_shared_kernel: one thread owns one line; its window of solution
+// values is two register arrays (previous / current element) with every index
+// known at compile time, so the inner products are fully unrolled FMAs with no
+// local memory.  The factor block of one element (BW1 rows x 2*BW1 padded
+// columns, 16*BW1^2 bytes) is the same for all lines of the CTA: it is staged
+// into shared memory with cp.async, double-buffered so the copy of element
+// ev+1 overlaps the arithmetic of element ev, and read back as warp broadcasts.
 #include "atb_generic.cuh"
 
 #include <type_traits>
@@ -186,142 +195,6 @@ __global__ void block_prep_kernel(const double* band, int KV, int BW1, double* b
   }
 }
 
-// One thread per (node kv of the element column, line l): it owns the NS rows
-// kv*NS .. kv*NS+NS-1 of every element block of its line.  Per element it
-// reads the line's right-hand-side / previous-solution vectors (2*BW1 values,
-// shared by its NS rows) and its NS rows of the two matrices (warp-uniform
-// addresses -> broadcasts, two doubles per load), and issues NS*2*BW1 FMAs.
-// Warps hold 32 lines at the same kv, so the global accesses of a state
-// component are consecutive addresses.
-template <int NQ, int NS, int LPB>
-__global__ void __launch_bounds__(NQ * LPB) band_solve_block_kernel(const BandSolve B, const double* blk) {
-  constexpr int BW1 = NQ * NS;
-  constexpr int MAT = BW1 * BW1;
-  extern __shared__ __align__(16) double sm[];
-  // smat(b): [Li|G] or [Ui|H], double-buffered (arithmetic, not a pointer
-  // array: a runtime-indexed local array would live in local memory)
-  auto smat = [&](int b) { return sm + b * 2 * MAT; };
-  double* ys = sm + 4 * MAT;             // [2][BW1][LPB]
-  double* bs = ys + 2 * BW1 * LPB;       // [BW1][LPB]
-  const LineMap& M = B.M;
-  const int l = threadIdx.x % LPB, kv = threadIdx.x / LPB;
-  const int line = blockIdx.x * LPB + l;
-  const bool act = line < M.nlines;
-  const int KV = M.KV, nh = M.nh, Np = M.Np;
-  const int hn = act ? line % nh : 0;
-  const int e0 = act ? M.e0[line] : 0;
-  const int nthr = NQ * LPB;
-  auto stage = [&](double* dst, const double* src) {
-    for (int c = threadIdx.x; c < MAT; c += nthr) cp_async16(dst + 2 * c, src + 2 * c);  // 2*MAT doubles
-  };
-  auto gidx = [&](int ev) { return (size_t)(e0 + ev * M.estep) * Np + hn + (size_t)nh * kv; };
-  // y_e = A_e v_e - C_e w_e-1 for this thread's NS rows (A, C row-major BW1 x BW1)
-  auto block_rows = [&](const double* Am, const double* Cm, const double* v, const double* w, double* out) {
-#pragma unroll
-    for (int s = 0; s < NS; ++s) out[s] = 0.0;
-    double acc2[NS];
-#pragma unroll
-    for (int s = 0; s < NS; ++s) acc2[s] = 0.0;
-#pragma unroll
-    for (int k = 0; k < BW1; ++k) {
-      const double vk = v[k * LPB + l], wk = w[k * LPB + l];
-#pragma unroll
-      for (int s = 0; s < NS; ++s) {
-        const int row = kv * NS + s;
-        out[s] += Am[row * BW1 + k] * vk;
-        acc2[s] += Cm[row * BW1 + k] * wk;
-      }
-    }
-#pragma unroll
-    for (int s = 0; s < NS; ++s) out[s] -= acc2[s];
-  };
-  // ------------------------------------------------------------ forward
-  stage(smat(0), blk);
-  cp_async_commit();
-  if (KV > 1) stage(smat(1), blk + (size_t)4 * MAT);
-  cp_async_commit();
-#pragma unroll
-  for (int s = 0; s < NS; ++s) {
-    ys[(kv * NS + s) * LPB + l] = 0.0;  // y_{-1} = 0
-    ys[BW1 * LPB + (kv * NS + s) * LPB + l] = 0.0;
-  }
-  double bnext[NS];
-  auto rhs = [&](int ev, double* b) {
-    const size_t g = gidx(ev);
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      double v = 0.0;
-      if (act) {
-        v = B.q[s][g];
-        // static pair index: the kernel-parameter pointer tables stay in the
-        // constant bank instead of being copied to local memory
-#pragma unroll
-        for (int k = 0; k < 2; ++k)
-          if (k < B.npairs) v = v + B.dt * (B.a[k] * B.ex[k][s][g] + B.b[k] * B.im[k][s][g]);
-      }
-      b[s] = v;
-    }
-  };
-  rhs(0, bnext);
-  for (int ev = 0; ev < KV; ++ev) {
-#pragma unroll
-    for (int s = 0; s < NS; ++s) bs[(kv * NS + s) * LPB + l] = bnext[s];
-    if (ev + 1 < KV) rhs(ev + 1, bnext);
-    cp_async_wait1();
-    __syncthreads();
-    double y[NS];
-    block_rows(smat(ev & 1), smat(ev & 1) + MAT, bs, ys + ((ev + 1) & 1) * BW1 * LPB, y);
-    const size_t g = gidx(ev);
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      ys[(ev & 1) * BW1 * LPB + (kv * NS + s) * LPB + l] = y[s];
-      if (act) B.out[s][g] = y[s];
-    }
-    __syncthreads();
-    if (ev + 2 < KV) stage(smat(ev & 1), blk + (size_t)(ev + 2) * 4 * MAT);
-    cp_async_commit();
-  }
-  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-  __syncthreads();
-  // ----------------------------------------------------------- backward
-  stage(smat(0), blk + (size_t)(KV - 1) * 4 * MAT + 2 * MAT);
-  cp_async_commit();
-  if (KV > 1) stage(smat(1), blk + (size_t)(KV - 2) * 4 * MAT + 2 * MAT);
-  cp_async_commit();
-#pragma unroll
-  for (int s = 0; s < NS; ++s) {
-    ys[(kv * NS + s) * LPB + l] = 0.0;
-    ys[BW1 * LPB + (kv * NS + s) * LPB + l] = 0.0;
-  }
-  double ynext[NS];
-  auto yload = [&](int ev, double* yv) {
-    const size_t g = gidx(ev);
-#pragma unroll
-    for (int s = 0; s < NS; ++s) yv[s] = act ? B.out[s][g] : 0.0;
-  };
-  yload(KV - 1, ynext);
-  for (int t = 0; t < KV; ++t) {
-    const int ev = KV - 1 - t;
-#pragma unroll
-    for (int s = 0; s < NS; ++s) bs[(kv * NS + s) * LPB + l] = ynext[s];
-    if (ev > 0) yload(ev - 1, ynext);
-    cp_async_wait1();
-    __syncthreads();
-    double x[NS];
-    block_rows(smat(t & 1), smat(t & 1) + MAT, bs, ys + ((t + 1) & 1) * BW1 * LPB, x);
-    const size_t g = gidx(ev);
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      ys[(t & 1) * BW1 * LPB + (kv * NS + s) * LPB + l] = x[s];
-      if (act) B.out[s][g] = x[s];
-    }
-    __syncthreads();
-    if (ev - 2 >= 0) stage(smat(t & 1), blk + (size_t)(ev - 2) * 4 * MAT + 2 * MAT);
-    cp_async_commit();
-  }
-  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-}
-
 typedef void (*solve_fn)(const BandSolve&, cudaStream_t);
 
 template <int NQ, int NS> void solve_launch(const BandSolve& B, cudaStream_t st) {
@@ -349,17 +222,6 @@ template <int NS> solve_fn pick_nq(int nq) {
   return nullptr;
 }
 
-
-template <int NQ, int NS> void block_launch(const BandSolve& B, cudaStream_t st) {
-  constexpr int BW1 = NQ * NS;
-  constexpr int LPB = 32;
-  constexpr size_t smem = sizeof(double) * (4 * BW1 * BW1 + 3 * BW1 * LPB);
-  static bool configured = false;
-  if (!configured && smem > 48 * 1024)
-    cudaFuncSetAttribute(band_solve_block_kernel<NQ, NS, LPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  configured = true;
-  band_solve_block_kernel<NQ, NS, LPB><<<(B.M.nlines + LPB - 1) / LPB, NQ * LPB, smem, st>>>(B, B.blk);
-}
 
 // Row-parallel form of the block recurrence: one thread per (row, line),
 // rows = the BW1 unknowns (node kv, state s) of one element of a vertical line,
@@ -1108,19 +970,6 @@ template <int NS> solve_fn pick_mma(int nq) {
     case 6: return mma_launch<6, NS>;
     case 7: return mma_launch<7, NS>;
     case 8: return mma_launch<8, NS>;
-  }
-  return nullptr;
-}
-
-template <int NS> solve_fn pick_block(int nq) {
-  switch (nq) {
-    case 2: return block_launch<2, NS>;
-    case 3: return block_launch<3, NS>;
-    case 4: return block_launch<4, NS>;
-    case 5: return block_launch<5, NS>;
-    case 6: return block_launch<6, NS>;
-    case 7: return block_launch<7, NS>;
-    case 8: return block_launch<8, NS>;
   }
   return nullptr;
 }
