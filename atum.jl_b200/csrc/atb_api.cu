@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -1036,11 +1037,13 @@ int build_band(atb_solver* s, cudaStream_t st) {
     if ((rc = dalloc(&s->blk, (size_t)M.KV * 4 * BW1 * BW1))) return rc;
     launch_block_prep(s->band, M.KV, BW1, s->blk, st);
     // the tile-sparse warp-owned solve, when the blocks have its zero structure
-    // (vertical coupling through face nodes only)
+    // (vertical coupling through face nodes only); ATB_BAND_DENSE=1 in the
+    // environment keeps the dense-block kernel (the tests compare the two)
     std::vector<double> hblk((size_t)M.KV * 4 * BW1 * BW1);
     CK(cudaMemcpyAsync(hblk.data(), s->blk, hblk.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    if (warp_solve_structure_ok(hblk.data(), M.KV, BW1, M.ns)) {
+    const char* dense = std::getenv("ATB_BAND_DENSE");
+    if (!(dense && dense[0] == '1') && warp_solve_structure_ok(hblk.data(), M.KV, BW1, M.ns)) {
       if ((rc = dalloc(&s->frag, frag_doubles(M.KV, BW1, M.ns)))) return rc;
       launch_frag_prep(s->blk, M.KV, BW1, M.ns, s->frag, st);
     }
