@@ -145,9 +145,14 @@ struct atb_op {
   std::vector<int> col_e0;    // bottom element of every vertical column
   bool cols_uniform = true;   // every instance has the same element counts
   int npre = 0, npv = 0;
-  void* h_geo = nullptr;        // page-locked geometry staging (pools)
-  size_t geo_bytes = 0;
-  cudaEvent_t geo_ev = nullptr;  // last copy out of h_geo
+  // page-locked geometry staging of pools: a ring of kGeoRing areas, each
+  // reused once the copies out of it have run, so a placement waits only for
+  // the copies of the placement kGeoRing before it
+  static constexpr int kGeoRing = 8;
+  void* h_geo[kGeoRing] = {};
+  size_t geo_bytes[kGeoRing] = {};
+  cudaEvent_t geo_ev[kGeoRing] = {};  // last copy out of h_geo[i]
+  int geo_turn = 0;
   std::vector<double> w, D;
   double* d_ginv = nullptr;
   int* d_nbr = nullptr;
@@ -306,11 +311,13 @@ extern "C" int atb_op_destroy(atb_op* op) {
   cudaFree(op->d_partials);
   cudaFree(op->d_red);
   if (op->h_red) cudaFreeHost(op->h_red);
-  if (op->geo_ev) {
-    cudaEventSynchronize(op->geo_ev);
-    cudaEventDestroy(op->geo_ev);
+  for (int i = 0; i < atb_op::kGeoRing; ++i) {
+    if (op->geo_ev[i]) {
+      cudaEventSynchronize(op->geo_ev[i]);
+      cudaEventDestroy(op->geo_ev[i]);
+    }
+    if (op->h_geo[i]) cudaFreeHost(op->h_geo[i]);
   }
-  if (op->h_geo) cudaFreeHost(op->h_geo);
   delete op;
   return ATB_OK;
 }
@@ -630,11 +637,12 @@ extern "C" int atb_op_create_pool(const atb_op_desc* kind, int capacity_elements
   if (rc) return rc;
   (*out)->K_active = 0;
   (*out)->col_e0.clear();
-  if (cudaEventCreateWithFlags(&(*out)->geo_ev, cudaEventDisableTiming) != cudaSuccess) {
-    atb_op_destroy(*out);
-    *out = nullptr;
-    return fail(ATB_ERR_CUDA, "event creation failed");
-  }
+  for (int i = 0; i < atb_op::kGeoRing; ++i)
+    if (cudaEventCreateWithFlags(&(*out)->geo_ev[i], cudaEventDisableTiming) != cudaSuccess) {
+      atb_op_destroy(*out);
+      *out = nullptr;
+      return fail(ATB_ERR_CUDA, "event creation failed");
+    }
   (*out)->cols_uniform = false;  // placements have their own grids: no banded solve
   return ATB_OK;
 }
@@ -654,28 +662,30 @@ extern "C" int atb_op_place_instance(atb_op* op, int first_element, const atb_op
     return fail(ATB_ERR_INVALID, "placement [%d, %ld) outside the pool's %d elements", first_element,
                 (long)first_element + Ki, op->K);
   if (op->naux > 0 && !aux_host) return fail(ATB_ERR_INVALID, "aux fields missing");
-  if (!op->geo_ev) return fail(ATB_ERR_INVALID, "instances are placed into pools (atb_op_create_pool)");
+  if (!op->geo_ev[0]) return fail(ATB_ERR_INVALID, "instances are placed into pools (atb_op_create_pool)");
   cudaStream_t st = (cudaStream_t)stream;
-  // geometry through the pool's page-locked staging area (reused once the
-  // previous placement's copies have run): no pageable copy that could block
-  // the caller behind queued work
+  // geometry through the next page-locked staging area of the ring: no
+  // pageable copy that could block the caller behind queued work, and a wait
+  // only for the copies of the placement kGeoRing placements ago (the copy
+  // stream also carries every placement's aux and state)
+  const int gi = op->geo_turn;
+  op->geo_turn = (gi + 1) % atb_op::kGeoRing;
   const size_t gbytes = (size_t)Ki * (4 * sizeof(double) + 6 * sizeof(int));
-  if (op->geo_bytes < gbytes) {
-    if (op->h_geo) {
-      CK(cudaEventSynchronize(op->geo_ev));
-      cudaFreeHost(op->h_geo);
-      op->h_geo = nullptr;
+  CK(cudaEventSynchronize(op->geo_ev[gi]));
+  if (op->geo_bytes[gi] < gbytes) {
+    if (op->h_geo[gi]) {
+      cudaFreeHost(op->h_geo[gi]);
+      op->h_geo[gi] = nullptr;
     }
-    if (cudaHostAlloc(&op->h_geo, gbytes, cudaHostAllocDefault) != cudaSuccess) {
-      op->h_geo = nullptr;
-      op->geo_bytes = 0;
-      return fail(ATB_ERR_NOMEM, "page-locked geometry staging of %zu bytes failed", gbytes);
+    const size_t want = std::max(gbytes, (size_t)1 << 20);
+    if (cudaHostAlloc(&op->h_geo[gi], want, cudaHostAllocDefault) != cudaSuccess) {
+      op->h_geo[gi] = nullptr;
+      op->geo_bytes[gi] = 0;
+      return fail(ATB_ERR_NOMEM, "page-locked geometry staging of %zu bytes failed", want);
     }
-    op->geo_bytes = gbytes;
-  } else {
-    CK(cudaEventSynchronize(op->geo_ev));
+    op->geo_bytes[gi] = want;
   }
-  double* ginv = (double*)op->h_geo;
+  double* ginv = (double*)op->h_geo[gi];
   double* J = ginv + (size_t)Ki * 3;
   int* nbr = (int*)(J + Ki);
   if (instance_geometry(desc, first_element, ginv, J, nbr, nullptr))
@@ -685,7 +695,7 @@ extern "C" int atb_op_place_instance(atb_op* op, int first_element, const atb_op
   CK(cudaMemcpyAsync(op->d_J + first_element, J, (size_t)Ki * sizeof(double), cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(op->d_nbr + (size_t)first_element * 6, nbr, (size_t)Ki * 6 * sizeof(int),
                      cudaMemcpyHostToDevice, st));
-  CK(cudaEventRecord(op->geo_ev, st));
+  CK(cudaEventRecord(op->geo_ev[gi], st));
   // aux: a pageable source is staged before the call returns; a page-locked
   // one is read by the copy engine later and must outlive the copies
   const size_t n = (size_t)Ki * op->Np;

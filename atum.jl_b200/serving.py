@@ -163,9 +163,37 @@ class _Staging:
         return b
 
 
+class _ResultBuffers:
+    """Page-locked host buffers for result copies, taken by a tick and given
+    back once ``poll`` has read them (page-locking memory is slow; a buffer per
+    tick cost tens of milliseconds of host time)."""
+
+    def __init__(self):
+        self.free = []
+
+    def get(self, n: int):
+        import torch
+
+        best = None
+        for b in self.free:
+            if b.numel() >= n and (best is None or b.numel() < best.numel()):
+                best = b
+        if best is not None:
+            self.free.remove(best)
+            return best
+        size = 1 << 23  # 64 MB of doubles at least, powers of two
+        while size < n:
+            size *= 2
+        return torch.empty(size, dtype=torch.float64, pin_memory=True)
+
+    def put(self, b):
+        if b is not None:
+            self.free.append(b)
+
+
 class _Pool:
     def __init__(self, key, template, capacity: int, chunk: int, kind: str, max_tick_steps: int,
-                 copy_stream=None, staging=None):
+                 copy_stream=None, staging=None, results=None):
         import torch
 
         from .odesolvers import Solver
@@ -188,6 +216,7 @@ class _Pool:
         # pool's launches; the pool stream waits for those copies
         self.copy_stream = copy_stream if copy_stream is not None else torch.cuda.Stream(device=self.cuda)
         self.staging = staging if staging is not None else _Staging()
+        self.results = results if results is not None else _ResultBuffers()
         self.pending = []
         self.q = torch.zeros((self.ns, self.capacity, self.Np), dtype=torch.float64, device=self.cuda)
         self.solver = Solver(kind, self, 1.0)
@@ -348,7 +377,7 @@ class _Pool:
         buf = None
         if fin:
             tot = sum(self.ns * p.K * self.Np for p in fin)
-            buf = torch.empty(tot, dtype=torch.float64, pin_memory=True)
+            buf = self.results.get(tot)
             o = 0
             with torch.cuda.stream(self.stream):
                 for p in fin:
@@ -412,6 +441,7 @@ class _Pool:
                 r.result = v.numpy().copy() if r.keep_result else None
                 r.finished = t
                 done.append(r)
+            self.results.put(buf)
             k += 1
         if not self.inflight:
             self.inflight_prefix = 0
@@ -454,6 +484,7 @@ class Server:
         self.max_inflight = 2
         self._copy_stream = None
         self._staging = _Staging()
+        self._results = _ResultBuffers()
         self.timers = {"admit": 0.0, "new_pool": 0.0, "tick": 0.0, "poll": 0.0, "release": 0.0}
         self.chunk = int(chunk)
         self.kind = kind
@@ -509,7 +540,8 @@ class Server:
 
         if self._copy_stream is None:
             self._copy_stream = torch.cuda.Stream()
-        p = _Pool(key, r.dg, cap, self.chunk, self.kind, self.max_tick_steps, self._copy_stream, self._staging)
+        p = _Pool(key, r.dg, cap, self.chunk, self.kind, self.max_tick_steps, self._copy_stream, self._staging,
+                  self._results)
         self.timers["new_pool"] += time.perf_counter() - t
         self.pools_made += 1
         self.pools.setdefault(key, []).append(p)
@@ -601,3 +633,4 @@ class Server:
         self.pools.clear()
         self.pool_bytes = 0
         torch.cuda.synchronize()
+        self._results.free.clear()

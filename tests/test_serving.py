@@ -81,6 +81,25 @@ def test_poisson_arrivals_realtime():
     srv.close()
 
 
+def test_many_placements_and_reused_result_buffers():
+    """More placements than the pool's ring of geometry staging areas, and more
+    finishing ticks than result buffers: every result still equals the
+    request stepped alone."""
+    base = _reqs(seed=11)
+    reqs = []
+    for k in range(4):
+        for r in base:
+            reqs.append(A.serving.Request(rid=len(reqs), dg=r.dg, q0=r.q0, dt=r.dt, nsteps=r.nsteps + k,
+                                          arrival=0.0))
+    assert len(reqs) > 8
+    srv = A.serving.Server(hbm_budget_bytes=2e9, capacity=4096, chunk=64, use_graphs=True)
+    st = srv.run(reqs, realtime=False)
+    srv.close()
+    assert st.requests == len(reqs) and st.ticks > 8
+    for r in reqs:
+        assert np.array_equal(r.result, _alone(r))
+
+
 def test_budget_too_small_raises():
     reqs = _requests(1)
     srv = A.serving.Server(hbm_budget_bytes=1.0, capacity=64)
