@@ -85,7 +85,7 @@ def test_many_placements_and_reused_result_buffers():
     """More placements than the pool's ring of geometry staging areas, and more
     finishing ticks than result buffers: every result still equals the
     request stepped alone."""
-    base = _reqs(seed=11)
+    base = _requests(6, seed=11)
     reqs = []
     for k in range(4):
         for r in base:
