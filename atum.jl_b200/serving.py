@@ -174,13 +174,12 @@ class _ResultBuffers:
     def get(self, n: int):
         import torch
 
-        best = None
-        for b in self.free:
-            if b.numel() >= n and (best is None or b.numel() < best.numel()):
-                best = b
-        if best is not None:
-            self.free.remove(best)
-            return best
+        best = -1
+        for i, b in enumerate(self.free):
+            if b.numel() >= n and (best < 0 or b.numel() < self.free[best].numel()):
+                best = i
+        if best >= 0:
+            return self.free.pop(best)  # by position: tensors compare element-wise
         size = 1 << 23  # 64 MB of doubles at least, powers of two
         while size < n:
             size *= 2
