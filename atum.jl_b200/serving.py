@@ -163,31 +163,37 @@ class _Staging:
         return b
 
 
-class _ResultBuffers:
-    """Page-locked host buffers for result copies, taken by a tick and given
-    back once ``poll`` has read them (page-locking memory is slow; a buffer per
-    tick cost tens of milliseconds of host time)."""
+class _ResultArena:
+    """One page-locked host arena for result copies, allocated once (page-
+    locking costs a few hundred milliseconds per gigabyte, far too much per
+    tick); a tick takes a first-fit region and ``poll`` gives it back after
+    reading it.  When no region fits, the tick gets a buffer of its own."""
 
-    def __init__(self):
-        self.free = []
+    def __init__(self, nbytes: float = 4e9):
+        self.n = int(nbytes) // 8
+        self.buf = None
+        self.used = []  # sorted (start, end) in doubles
+        self.fallbacks = 0
 
     def get(self, n: int):
+        """(tensor view of n doubles, token for ``put``)."""
         import torch
 
-        best = -1
-        for i, b in enumerate(self.free):
-            if b.numel() >= n and (best < 0 or b.numel() < self.free[best].numel()):
-                best = i
-        if best >= 0:
-            return self.free.pop(best)  # by position: tensors compare element-wise
-        size = 1 << 23  # 64 MB of doubles at least, powers of two
-        while size < n:
-            size *= 2
-        return torch.empty(size, dtype=torch.float64, pin_memory=True)
+        if self.buf is None and n <= self.n:
+            self.buf = torch.empty(self.n, dtype=torch.float64, pin_memory=True)
+        if self.buf is not None:
+            start = 0
+            for k, (a, b) in enumerate(self.used + [(self.n, self.n)]):
+                if a - start >= n:
+                    self.used.insert(k, (start, start + n))
+                    return self.buf[start:start + n], (start, start + n)
+                start = b
+        self.fallbacks += 1
+        return torch.empty(n, dtype=torch.float64, pin_memory=True), None
 
-    def put(self, b):
-        if b is not None:
-            self.free.append(b)
+    def put(self, token):
+        if token is not None:
+            self.used.remove(token)
 
 
 class _Pool:
@@ -215,7 +221,7 @@ class _Pool:
         # pool's launches; the pool stream waits for those copies
         self.copy_stream = copy_stream if copy_stream is not None else torch.cuda.Stream(device=self.cuda)
         self.staging = staging if staging is not None else _Staging()
-        self.results = results if results is not None else _ResultBuffers()
+        self.results = results if results is not None else _ResultArena()
         self.pending = []
         self.q = torch.zeros((self.ns, self.capacity, self.Np), dtype=torch.float64, device=self.cuda)
         self.solver = Solver(kind, self, 1.0)
@@ -376,7 +382,7 @@ class _Pool:
         buf = None
         if fin:
             tot = sum(self.ns * p.K * self.Np for p in fin)
-            buf = self.results.get(tot)
+            buf, token = self.results.get(tot)
             o = 0
             with torch.cuda.stream(self.stream):
                 for p in fin:
@@ -392,7 +398,7 @@ class _Pool:
         ev = self.stream.record_event()
         self.host["dt"] += t1 - t0
         self.host["launch"] += t2 - t1
-        self.inflight.append((ev, outs, buf))
+        self.inflight.append((ev, outs, (buf, token) if fin else None))
         return S
 
     def _compact(self):
@@ -429,7 +435,7 @@ class _Pool:
         when ``wait``); returns how many completed."""
         k = 0
         while self.inflight:
-            ev, outs, buf = self.inflight[0]
+            ev, outs, held = self.inflight[0]
             if not ev.query():
                 if not (wait and k == 0):
                     break
@@ -440,7 +446,8 @@ class _Pool:
                 r.result = v.numpy().copy() if r.keep_result else None
                 r.finished = t
                 done.append(r)
-            self.results.put(buf)
+            if held is not None:
+                self.results.put(held[1])
             k += 1
         if not self.inflight:
             self.inflight_prefix = 0
@@ -466,13 +473,17 @@ class Server:
 
     def __init__(self, hbm_budget_bytes: float = 150e9, capacity: Optional[int] = None, chunk: int = 256,
                  kind: str = "LSRK54", max_tick_steps: int = 16, use_graphs: bool = True,
-                 pool_bytes: Optional[float] = None, max_pool_elements: int = 1 << 18):
+                 pool_bytes: Optional[float] = None, max_pool_elements: int = 1 << 18,
+                 result_bytes: float = 2e9):
         """``capacity``: elements per pool (fixed); otherwise a pool holds
         ``pool_bytes`` (default: an eighth of the budget) worth of elements of
         its kind, at most ``max_pool_elements`` and at least the request that
         opens it.  Inputs held in page-locked host memory (``pinned_array``)
         are copied by DMA straight from the caller's buffer, which must stay
-        unchanged while the server runs; others go through pinned staging."""
+        unchanged while the server runs; others go through pinned staging.
+        ``result_bytes``: the page-locked host arena that results are copied
+        into (allocated at the first result; a tick whose results do not fit
+        gets a buffer of its own, which is slow to allocate)."""
         if kind not in _KIND_STAGES:
             raise ValueError("the server steps with LSRK54 or LSRK144")
         self.budget = float(hbm_budget_bytes)
@@ -483,7 +494,8 @@ class Server:
         self.max_inflight = 2
         self._copy_stream = None
         self._staging = _Staging()
-        self._results = _ResultBuffers()
+        self.result_bytes = float(result_bytes)
+        self._results = _ResultArena(self.result_bytes)
         self.timers = {"admit": 0.0, "new_pool": 0.0, "tick": 0.0, "poll": 0.0, "release": 0.0}
         self.chunk = int(chunk)
         self.kind = kind
@@ -617,6 +629,7 @@ class Server:
         st.ticks = ticks
         st.extra["dof_stage_updates"] = int(total)
         st.extra["host_seconds"] = dict(self.timers)
+        st.extra["result_arena_fallbacks"] = self._results.fallbacks
         for ps in self.pools.values():
             for p in ps:
                 for k, v in p.host.items():
@@ -632,4 +645,4 @@ class Server:
         self.pools.clear()
         self.pool_bytes = 0
         torch.cuda.synchronize()
-        self._results.free.clear()
+        self._results = _ResultArena(self.result_bytes)

@@ -530,7 +530,7 @@ def run_serve(args):
     for r in sampled:
         r.keep_result = True
     srv = A.serving.Server(hbm_budget_bytes=args.hbm_budget_gb * 1e9, chunk=256, use_graphs=True,
-                           pool_bytes=args.pool_gb * 1e9)
+                           pool_bytes=args.pool_gb * 1e9, result_bytes=args.result_gb * 1e9)
     # warm-up stream (a few requests), then the measured one
     warm = [A.serving.Request(rid=-1 - j, dg=r.dg, q0=r.q0, dt=r.dt, nsteps=min(r.nsteps, 4), arrival=0.0,
                               keep_result=False) for j, r in enumerate(reqs[:args.warmup])]
@@ -571,6 +571,7 @@ def run_serve(args):
         "makespan_s": st.makespan_s, "arrival_window_s": max(r.arrival for r in reqs),
         "pools": st.pools, "ticks": st.ticks,
         "host_seconds": st.extra["host_seconds"],
+        "result_arena_fallbacks": st.extra.get("result_arena_fallbacks"),
         "peak_pool_bytes": st.peak_pool_bytes, "dof_stage_updates": st.extra["dof_stage_updates"],
         "rel_l2_vs_fp64": {"samples": len(errs), "max": max(errs) if errs else None,
                            "median": float(np.median(errs)) if errs else None},
@@ -937,6 +938,8 @@ def main():
     ap.add_argument("--time-scale", type=float, default=0.0005)
     ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
     ap.add_argument("--pool-gb", type=float, default=12.0)
+    ap.add_argument("--result-gb", type=float, default=16.0,
+                    help="serve: page-locked host arena for result copies")
     ap.add_argument("--error-samples", type=int, default=16)
     args = ap.parse_args()
     if args.warmup < 3:
