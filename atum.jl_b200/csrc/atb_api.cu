@@ -560,8 +560,9 @@ int op_create_impl(const atb_op_desc* descs, int n, const double* const* aux_hos
   while (op->E > 1 && op_smem(op, op->E) > 100 * 1024) --op->E;
   op->smem = op_smem(op, op->E);
   if (op->smem > 227 * 1024) {
+    const size_t smem = op->smem;
     delete op;
-    return fail(ATB_ERR_INVALID, "element too large for shared memory (%zu bytes)", op->smem);
+    return fail(ATB_ERR_INVALID, "element too large for shared memory (%zu bytes)", smem);
   }
   op->red_blocks = 148 * 4;
   int rc;
