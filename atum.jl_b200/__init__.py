@@ -6,9 +6,9 @@ ARK23 solvers) behind a C ABI (``include/atum_b200.h``).  This package is the
 host-side mirror of the reference's Julia API; the compute runs in the CUDA
 library ``csrc/libatumb200.so`` and there is no CPU fallback.
 
-The directory name is not a Python identifier: load it with
-``atum_b200.load()`` from ``__graft_entry__`` or put its parent on the path and
-use ``importlib`` (see ``_load_package`` in ``__graft_entry__.py``).
+The directory name is not a Python identifier: load it as ``atum_b200`` with
+``_load_package()`` from ``__graft_entry__.py`` at the repository root (an
+``importlib`` spec over this directory; the tests do the same in conftest).
 """
 from .cell import LobattoCell, BrickGrid, brickgrid, min_node_distance, points
 from .laws import (AbstractProblem, DummyProblem, ReflectiveWall, InflowZero, DirichletByTag, Coriolis,
