@@ -103,3 +103,19 @@ def test_set_state_rejects_non_finite():
         s.set_state(float("nan"), 1.0)
     s.set_state(2.5, 1.0)
     assert s.time == 2.5
+
+
+def test_resume_restores_dt_and_state():
+    class S:
+        kind = "LSRK54"
+        dt = 1e-3
+        calls = []
+
+        def set_state(self, time, gamma):
+            self.calls.append((time, gamma))
+
+    s = S()
+    CK.resume(s, {"solver": {"kind": "LSRK54", "time": 2.5, "dt": 2e-3, "gamma": 0.75}})
+    assert s.dt == 2e-3 and s.calls == [(2.5, 0.75)]
+    with pytest.raises(ValueError, match="RLSRK54"):
+        CK.resume(s, {"solver": {"kind": "RLSRK54", "time": 0.0, "dt": 2e-3, "gamma": 1.0}})

@@ -48,3 +48,20 @@ def test_two_gloo_ranks():
         assert work == 300.0
         flat = [s for rs in everyone for s in rs]
         assert len(flat) == len(set(flat)) == 8
+
+
+def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
+    """Under torchrun every rank starts the reference arm; ranks other than 0
+    return at once, with no output and no work."""
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    import bench
+    monkeypatch.setenv("RANK", "1")
+    monkeypatch.setenv("WORLD_SIZE", "2")
+
+    class Args:
+        scheme, steps, warmup = "ark23", 1, 3
+
+    assert bench.run_reference(Args()) == 0
+    assert capsys.readouterr().out == ""
