@@ -23,7 +23,8 @@ __version__ = "0.1.0"
 
 def __getattr__(name):
     # solvers / measures / serving import torch and the CUDA library lazily
-    if name in ("measures", "odesolvers", "serving", "batch", "_lib", "_device", "build", "checkpoint", "vtk"):
+    if name in ("measures", "odesolvers", "serving", "batch", "_lib", "_device", "build", "checkpoint", "vtk",
+                "workloads"):
         import importlib
         return importlib.import_module("." + name, __name__)
     if name in ("LSRK54", "LSRK144", "RLSRK54", "RLSRK144", "ARK23", "solve_", "LSRK", "RLSRK", "ARK"):

@@ -141,6 +141,7 @@ struct atb_op {
   atb_op_desc kind{};  // instance 0's descriptor (kind checks of later placements)
   int ninst = 1;      // instances packed into this operator
   int K_active = 0;   // elements the tendency launches cover (a prefix of K)
+  int device = -1;    // the CUDA device current at creation (its memory holds every buffer)
   std::vector<int> inst_off;  // first element of each instance, then K
   std::vector<int> col_e0;    // bottom element of every vertical column
   bool cols_uniform = true;   // every instance has the same element counts
@@ -448,6 +449,10 @@ int op_create_impl(const atb_op_desc* descs, int n, const double* const* aux_hos
     return fail(ATB_ERR_INVALID,
                 "the FP32-flux form exists for the flux-differencing volume term with the entropy-conservative "
                 "flux (Euler, Euler-gravity, shallow water) or the Kennedy-Gruber flux (Euler, Euler-gravity)");
+  if (d->precision == ATB_PREC_FP32FLUX && d->surface_flux != ATB_FLUX_CENTRAL && d->surface_flux != ATB_FLUX_RUSANOV)
+    return fail(ATB_ERR_INVALID,
+                "the FP32-flux form has FP32 arithmetic for the central and Rusanov surface fluxes only; "
+                "use precision FP64 with surface flux %d", d->surface_flux);
   tend_launch_fn fn = nullptr;
   red_launch_fn rf = nullptr;
   // a compile-time node-count specialisation when one exists, else the
@@ -473,7 +478,13 @@ int op_create_impl(const atb_op_desc* descs, int n, const double* const* aux_hos
   if ((d->law == LAW_LEG || (d->law == LAW_EG && d->pde_level_balance)) && d->naux < 3 + d->dim)
     return fail(ATB_ERR_INVALID, "this law needs the reference state in aux");
 
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ATB_ERR_CUDA, "no usable CUDA device");
+  }
   atb_op* op = new atb_op();
+  op->device = dev;
   op->launch = fn;
   op->reducer = rf;
   op->dim = d->dim;
@@ -1099,7 +1110,9 @@ int lsrk_steps(atb_solver* s, double* const* q, int nsteps, cudaStream_t st) {
     }
     s->time += s->dt;
   }
-  if (!in_user) return copy_field(q, cur, s->ns, s->stride, st);
+  // an odd number of stages leaves the state in qB: copy back the active
+  // elements (the kernel writes no others)
+  if (!in_user) return copy_field(q, cur, s->ns, (size_t)op->K_active * op->Np, st);
   return ATB_OK;
 }
 
@@ -1451,6 +1464,8 @@ extern "C" int atb_solver_create(int kind, atb_op* rhs, atb_op* linrhs, double d
   if (!out) return fail(ATB_ERR_INVALID, "null argument");
   *out = nullptr;
   if (kind < ATB_LSRK54 || kind > ATB_ARK23) return fail(ATB_ERR_INVALID, "unknown solver kind %d", kind);
+  if (!std::isfinite(dt) || !(dt > 0.0)) return fail(ATB_ERR_INVALID, "dt must be finite and positive (got %g)", dt);
+  if (!std::isfinite(t0)) return fail(ATB_ERR_INVALID, "t0 must be finite");
   if (kind != ATB_ARK23 && (!rhs || linrhs)) return fail(ATB_ERR_INVALID, "explicit solvers take rhs only");
   if (kind == ATB_ARK23 && !rhs && !linrhs) return fail(ATB_ERR_INVALID, "ARK23 needs rhs or linrhs");
   atb_op* any = rhs ? rhs : linrhs;
@@ -1534,6 +1549,7 @@ extern "C" int atb_solver_step(atb_solver* s, double* const* q, int nsteps, void
 extern "C" int atb_solve(atb_solver* s, double* const* q, double timeend, int adjust_final, int* steps_out,
                          void* stream) {
   if (!s || !q) return fail(ATB_ERR_INVALID, "bad argument");
+  if (!std::isfinite(timeend)) return fail(ATB_ERR_INVALID, "timeend must be finite");
   int step = 0;
   bool finalstep = false;
   while (true) {
@@ -1542,6 +1558,11 @@ extern "C" int atb_solve(atb_solver* s, double* const* q, double timeend, int ad
     if (time + s->dt >= timeend) {
       if (adjust_final) s->dt = timeend - time;
       finalstep = true;
+    } else if (!(time + s->dt > time)) {
+      // a step that does not advance the clock (dt <= 0, or below the clock's
+      // resolution) would never reach timeend
+      return fail(ATB_ERR_INVALID, "solve: dt = %g does not advance time %g towards timeend %g", s->dt, time,
+                  timeend);
     }
     int rc = do_steps(s, q, 1, (cudaStream_t)stream);
     if (rc) return rc;
@@ -1569,6 +1590,7 @@ extern "C" int atb_solver_set_state(atb_solver* s, double time, double gamma) {
 
 extern "C" int atb_solver_set_dt(atb_solver* s, double dt) {
   if (!s) return fail(ATB_ERR_INVALID, "null solver");
+  if (!std::isfinite(dt) || dt < 0.0) return fail(ATB_ERR_INVALID, "dt must be finite and non-negative (got %g)", dt);
   if (s->kind == ATB_ARK23 && s->lin && dt != s->dt)
     return fail(ATB_ERR_INVALID, "ARK23 factors I - dt a L for a fixed dt");
   s->dt = dt;
@@ -1694,6 +1716,7 @@ extern "C" int atb_op_instances(const atb_op* op, int* n, int* first_elements) {
 // LSRK(5,4) stages of `op` with caller-provided device scratch (dq and the
 // second state buffer): launches only, no allocation of any kind.
 int atb_detail_fail(int code, const char* msg) { return fail(code, "%s", msg); }
+int atb_detail_op_device(const atb_op* op) { return op->device; }
 
 int atb_detail_lsrk54_steps(atb_op* op, double* const* q, double* dqbuf, double* qbbuf, double dt, int nsteps,
                             cudaStream_t st) {
@@ -1712,7 +1735,10 @@ int atb_detail_lsrk54_steps(atb_op* op, double* const* q, double* dqbuf, double*
     oth[k] = qbbuf + (size_t)c * n;
   }
   bool in_user = true;
-  const int grid = (op->K + op->E - 1) / op->E;
+  // the same launches as the allocating path (run_tendency): the active
+  // element prefix only, nothing at all when it is empty
+  const int grid = (op->K_active + op->E - 1) / op->E;
+  if (grid == 0) return ATB_OK;
   for (int step = 0; step < nsteps; ++step)
     for (int i = 0; i < 5; ++i) {
       TendArgs A;
@@ -1721,14 +1747,20 @@ int atb_detail_lsrk54_steps(atb_op* op, double* const* q, double* dqbuf, double*
       A.a = rka[i];
       A.bdt = rkb[i] * dt;
       for (int k = 0; k < 5; ++k) { A.q[k] = cur[k]; A.out[k] = dq[k]; A.out2[k] = oth[k]; }
-      op->launch(A, grid, cta_threads(op->E, op->Np), op->smem, st);
+      {
+        ProfScope ps(op->prof_class, st);
+        op->launch(A, grid, cta_threads(op->E, op->Np), op->smem, st);
+      }
       const int rc = check_launch("tendency (no-alloc LSRK54)");
       if (rc) return rc;
       for (int k = 0; k < 5; ++k) std::swap(cur[k], oth[k]);
       in_user = !in_user;
     }
+  // after an odd number of stages the state is in the scratch buffer: copy
+  // back the active elements only (rows beyond them were never written)
   if (!in_user)
     for (int s = 0; s < ns; ++s)
-      CK(cudaMemcpyAsync(q[s], cur[s], n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      CK(cudaMemcpyAsync(q[s], cur[s], (size_t)op->K_active * op->Np * sizeof(double), cudaMemcpyDeviceToDevice,
+                         st));
   return ATB_OK;
 }

@@ -20,10 +20,12 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <mutex>
 
 struct atb_op;
 int atb_detail_fail(int code, const char* msg);
+int atb_detail_op_device(const atb_op* op);
 int atb_detail_lsrk54_steps(atb_op* op, double* const* q, double* dqbuf, double* qbbuf, double dt, int nsteps,
                             cudaStream_t st);
 
@@ -60,6 +62,17 @@ int scratch_on_current_device(double** out) {
 
 extern "C" int atb_lsrk54_step_noalloc(atb_op* op, double* const* q, double dt, int nsteps, void* stream) {
   if (!op || !q || nsteps < 0) return atb_detail_fail(ATB_ERR_INVALID, "atb_lsrk54_step_noalloc: bad argument");
+  if (!std::isfinite(dt)) return atb_detail_fail(ATB_ERR_INVALID, "atb_lsrk54_step_noalloc: dt is not finite");
+  // the scratch address is per device: with another device current it would
+  // point into memory the op's kernels cannot use
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return atb_detail_fail(ATB_ERR_CUDA, "atb_lsrk54_step_noalloc: no usable current device");
+  }
+  if (dev != atb_detail_op_device(op))
+    return atb_detail_fail(ATB_ERR_INVALID,
+                           "atb_lsrk54_step_noalloc: the current device is not the one the operator was created on");
   int ns = 0, K = 0, Np = 0;
   int rc = atb_op_dims(op, &ns, &K, &Np);
   if (rc) return rc;

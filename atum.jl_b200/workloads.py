@@ -1,0 +1,206 @@
+"""Workload builders of the benchmark configurations: seeded synthetic
+initial states on brick grids, restated from the reference's test and
+experiment setups (test/euler/isentropicvortex.jl:16-32,
+test/euler_gravity/linear.jl:20-43, experiment/euler_gravity/risingbubble.jl:10-15).
+
+Each builder returns a ``Case``: the DGSEM spec(s), the initial state, dt, end
+time, solver kind and the exact solution (when there is one).  ``bench.py``
+times these workloads; the tests drive the same builders through the CUDA
+library and the CPU oracle.
+
+* ``vortex_c1``   2-D Euler isentropic vortex, 8x8 elements, N=3, LSRK54
+* ``bubble_3d``   3-D Euler-gravity rising bubble, 16^3 elements, N=4, IMEX ARK23
+* ``sw_fplane``   rotating shallow water with bathymetry, 32^2 elements, N=4
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Callable, Optional
+
+import numpy as np
+
+from .dgsem import DGSEM
+from .laws import (EulerLaw, EulerGravityLaw, LinearEulerGravityLaw, ShallowWaterLaw, ReflectiveWall, Coriolis,
+                   RusanovFlux, EntropyConservativeFlux, KennedyGruberFlux, FluxDifferencingForm)
+from .cell import LobattoCell, brickgrid, min_node_distance
+
+
+@dataclass
+class Case:
+    name: str
+    dg: object
+    q0: np.ndarray
+    dt: float
+    timeend: float
+    solver: str = "LSRK54"
+    lindg: object = None
+    split_rhs: bool = True
+    adjust_final: bool = True
+    exact: Optional[Callable] = None
+    extra: dict = field(default_factory=dict)
+
+
+def _vec(lo, hi, K):
+    # Julia range(lo, stop=hi, length=K+1): values lo + i*(hi-lo)/K
+    return np.array([lo + (hi - lo) * i / K for i in range(K + 1)], dtype=np.float64)
+
+
+def _pack(*comps):
+    return np.ascontiguousarray(np.stack([np.broadcast_to(c, comps[0].shape) for c in comps]))
+
+
+
+def vortex_c1(N=3, K=8, steps=100, vflux="ec", precision="fp64"):
+    """Plain-method config: 2-D Euler isentropic vortex on periodic [-5,5]^2,
+    8x8 elements, N=3, rho=1, u=v=1, p=1, gamma=1.4, strength 5 at the origin,
+    EC volume flux, Rusanov surface flux, LSRK54, dt = 0.3 dx / N, 100 fixed
+    steps; analytic solution wrapped periodically (minimum image)."""
+    law = EulerLaw(2)
+    cell = LobattoCell(N + 1, N + 1)
+    v = _vec(-5.0, 5.0, K)
+    grid = brickgrid(cell, (v, v), periodic=(True, True))
+    vf = FluxDifferencingForm(EntropyConservativeFlux() if vflux == "ec" else KennedyGruberFlux())
+    dg = DGSEM(law=law, grid=grid, volume_form=vf, surface_numericalflux=RusanovFlux(), precision=precision)
+    dx = v[1] - v[0]
+    g = law.gamma
+
+    def vortex(x, t):
+        r0 = x[0] - 1.0 * t
+        r1 = x[1] - 1.0 * t
+        r0 = r0 - 10.0 * np.round(r0 / 10.0)
+        r1 = r1 - 10.0 * np.round(r1 / 10.0)
+        f = 5.0 * np.exp(1 - (r0 * r0 + r1 * r1))
+        rho = (1 - (g - 1) * f ** 2 / (16 * g * np.pi ** 2)) ** (1 / (g - 1))
+        u0 = 1.0 + f / (2 * np.pi) * (-r1)
+        u1 = 1.0 + f / (2 * np.pi) * r0
+        rhou = [rho * u0, rho * u1]
+        return _pack(rho, *rhou, law.energy(rho, rhou, rho ** g))
+
+    x = grid.points()
+    q0 = vortex(x, 0.0)
+    # CFL 0.3 in the reference tests' form dt = cfl * dx / N / speed, with the
+    # largest wave speed |u| + c of the initial state
+    rho, m, E = q0[0], q0[1:3], q0[3]
+    p = law.pressure(rho, list(m), E)
+    lam = float(np.max(np.sqrt(m[0] ** 2 + m[1] ** 2) / rho + np.sqrt(g * p / rho)))
+    dt = 0.3 * dx / N / lam
+    return Case("vortex_c1", dg, q0, dt, steps * dt, exact=lambda t: vortex(x, t), extra={"steps": steps})
+
+
+# --------------------------------------------------- 3-D Euler + gravity bubble
+def bubble_reference(law, x):
+    """Constant potential temperature (theta0 = 300 K) hydrostatic background."""
+    z = x[law.dim - 1]
+    cv_d = 719.0
+    cp_d = law.gamma * cv_d
+    R_d = cp_d - cv_d
+    theta = 300.0
+    p0 = 1e5
+    pi_exner = 1 - law.grav / (cp_d * theta) * z
+    rho = p0 / (R_d * theta) * pi_exner ** (cv_d / R_d)
+    p = p0 * pi_exner ** (cp_d / R_d)
+    return rho, p
+
+
+def bubble_3d(N=4, K=16, L=10e3, imex=True, steps=200, dt=None, precision="fp64", vflux="ec",
+              fd_kernel="per_dir"):
+    """3-D rising warm bubble: box L^3, K^3 hexahedra (K an int) or Kx x Ky x Kz
+    (K a 3-tuple), order N; constant-theta
+    hydrostatic background (theta0 = 300 K, g = 9.81), +2 K Gaussian theta
+    perturbation of 2 km radius centred 2 km above ground; periodic laterally,
+    reflective walls top/bottom.  IMEX ARK23 (split_rhs = false) with the
+    vertical acoustic terms implicit through the banded column solve, or
+    explicit LSRK54 at small dt.  ``fd_kernel`` picks the flux-differencing
+    schedule (``per_dir``, ``per_dir_symmetric``, ``naive``)."""
+    problem = ReflectiveWall(referencestate=bubble_reference)
+    law = EulerGravityLaw(3, grav=9.81, problem=problem)
+    cell = LobattoCell(N + 1, N + 1, N + 1)
+    Ks = tuple(K) if isinstance(K, (tuple, list)) else (K, K, K)
+    grid = brickgrid(cell, tuple(_vec(0.0, L, k) for k in Ks), periodic=(True, True, False), ordering="stacked")
+    vf = FluxDifferencingForm(EntropyConservativeFlux() if vflux == "ec" else KennedyGruberFlux(), fd_kernel)
+    dg = DGSEM(law=law, grid=grid, volume_form=vf, surface_numericalflux=RusanovFlux(), precision=precision)
+    x = grid.points()
+    aux = dg.auxstate_host()
+    Phi = aux[0]
+    cv_d = 719.0
+    cp_d = law.gamma * cv_d
+    R_d = cp_d - cv_d
+    r = np.sqrt((x[0] - L / 2) ** 2 + (x[1] - L / 2) ** 2 + (x[2] - 2000.0) ** 2)
+    dtheta = 2.0 * np.exp(-(r / 2000.0) ** 2)
+    theta = 300.0 + dtheta
+    z = x[2]
+    # keep the hydrostatic pressure, perturb temperature: rho = p / (R T)
+    pi_exner = 1 - law.grav / (cp_d * 300.0) * z
+    p = 1e5 * pi_exner ** (cp_d / R_d)
+    T = theta * pi_exner
+    rho = p / (R_d * T)
+    zero = np.zeros_like(rho)
+    rhoe = law.energy(rho, [zero] * 3, p, Phi)
+    q0 = _pack(rho, zero, zero, zero, rhoe)
+    dz = min_node_distance(grid, dims=(3,))
+    if imex:
+        lin = LinearEulerGravityLaw(law)
+        # the implicit vertical operator and its banded solve stay FP64 in
+        # every precision form
+        lindg = DGSEM(law=lin, grid=grid, surface_numericalflux=RusanovFlux(), auxstate=aux, directions=(3,))
+        # the box is isotropic: the explicit part's horizontal acoustic CFL sets dt
+        dt = dt if dt is not None else 0.25 * dz / 340.0
+        return Case("bubble_3d_imex", dg, q0, dt, steps * dt, solver="ARK23", lindg=lindg, split_rhs=False,
+                    adjust_final=False, extra={"steps": steps})
+    dt = dt if dt is not None else 0.3 * dz / 340.0
+    return Case("bubble_3d_lsrk", dg, q0, dt, steps * dt, extra={"steps": steps})
+
+
+# ------------------------------------------------------ shallow water, C3
+def sw_fplane(N=4, K=32, L=1.0e6, H=100.0, seed=20261203, lake_at_rest=False, precision="fp64", f=1e-4,
+              steps=500):
+    """Rotating shallow water (f-plane, g = 9.81) on a periodic square of K x K
+    elements, order N; smooth random bottom topography (sum of 8 Gaussians,
+    amplitude <= 10% of the mean depth H) and seeded random height
+    perturbations (amplitude 1 m, wavelengths 4-16 elements).  EC volume flux
+    with the well-balanced bathymetry terms, Rusanov surface flux, LSRK54."""
+    rng = np.random.default_rng(seed)
+    cell = LobattoCell(N + 1, N + 1)
+    v = _vec(0.0, L, K)
+    grid = brickgrid(cell, (v, v), periodic=(True, True))
+    g = 9.81
+    cx, cy = rng.uniform(0, L, 8), rng.uniform(0, L, 8)
+    amp = rng.uniform(-0.1 * H, 0.1 * H, 8) / 2
+    wid = rng.uniform(0.05 * L, 0.15 * L, 8)
+
+    def bath(x):
+        b = np.zeros(x.shape[1:])
+        gx, gy = np.zeros_like(b), np.zeros_like(b)
+        for i in range(8):
+            dx = (x[0] - cx[i] + L / 2) % L - L / 2
+            dy = (x[1] - cy[i] + L / 2) % L - L / 2
+            e = amp[i] * np.exp(-(dx * dx + dy * dy) / wid[i] ** 2)
+            b += e
+            gx += -2 * dx / wid[i] ** 2 * e
+            gy += -2 * dy / wid[i] ** 2 * e
+        return b, [gx, gy]
+
+    law = ShallowWaterLaw(2, grav=g, topography=True, problem=Coriolis((0.0, 0.0, f)))
+    law.bathymetry = bath
+    dg = DGSEM(law=law, grid=grid, volume_form=FluxDifferencingForm(EntropyConservativeFlux()),
+                 surface_numericalflux=RusanovFlux(), precision=precision)
+    x = grid.points()
+    b = dg.auxstate_host()[0]
+    eta = np.zeros_like(b)
+    if not lake_at_rest:
+        for _ in range(6):
+            wl = rng.uniform(4, 16) * (L / K)
+            th = rng.uniform(0, 2 * np.pi)
+            kx, ky = 2 * np.pi / wl * np.cos(th), 2 * np.pi / wl * np.sin(th)
+            # periodic: round the wavenumber to the box
+            kx = 2 * np.pi * np.round(kx * L / (2 * np.pi)) / L
+            ky = 2 * np.pi * np.round(ky * L / (2 * np.pi)) / L
+            eta += np.sin(kx * x[0] + ky * x[1] + rng.uniform(0, 2 * np.pi))
+        eta *= 1.0 / np.max(np.abs(eta))
+    h = H - b + eta
+    z = np.zeros_like(h)
+    q0 = _pack(h, z, z, h * 0.0)
+    dx = L / K
+    dt = 0.3 * dx / N / (np.sqrt(g * np.max(h)))
+    return Case("sw_fplane", dg, q0, dt, steps * dt, extra={"steps": steps})

@@ -38,7 +38,6 @@ import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
-sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 # Algorithmic FP64 flops per DOF-stage of the flux-differencing tendency
 # (EC volume flux, Rusanov surface flux), from the oracle's instrumented
@@ -121,7 +120,8 @@ SCHEME_STAGES = {"ark23": 3, "lsrk54": 5}
 def build_case(precision="fp64", K=16, scheme="ark23"):
     """The rising bubble: IMEX ARK23 with the vertical acoustics implicit, or
     the fully explicit LSRK54 run of the same problem at its smaller dt."""
-    import problems as P
+    load_pkg()
+    from atum_b200 import workloads as P
     return P.bubble_3d(N=4, K=K, imex=(scheme == "ark23"), steps=200, precision=precision)
 
 
@@ -141,6 +141,15 @@ def make_oracle_solver(orc, case, q, scheme):
 def scheme_label(scheme):
     return ("IMEX ARK23 split_rhs=false, vertical banded solve" if scheme == "ark23"
             else "explicit LSRK54 (Carpenter-Kennedy 5-stage)")
+
+
+def workload_config(scheme, precision="fp64"):
+    """The ``config`` dict both arms print for the rising-bubble workload
+    (identical, so the two lines name the same workload)."""
+    return {"workload": "3-D Euler-gravity rising bubble, 16^3 hexahedra, N=4 (2,560,000 DOFs), EC volume + "
+                        "Rusanov surface flux, " + scheme_label(scheme),
+            "dofs": 2560000, "stages_per_step": SCHEME_STAGES[scheme], "precision": precision,
+            "l2": "working set ~0.21 GB > 126 MB L2 (no flush)"}
 
 
 def dist_init():
@@ -224,8 +233,7 @@ def run_reference(args):
     line = {"metric": "DOF-stage updates/s", "value": v, "unit": "DOF-stage/s", "n_gpus": 0, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": T / args.steps * 1e3, "higher_is_better": True,
             "impl": "reference", "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"3-D Euler-gravity rising bubble, 16^3 hexahedra, N=4, FP64, "
-                                   f"{scheme_label(args.scheme)} (CPU)", "sample": sample},
+            "config": workload_config(args.scheme), "parallelism": f"{threads} host threads",
             "cpu_baseline": {"value": v, "unit": "DOF-stage/s", "cores": threads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": v, "unit": "DOF-stage/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -238,7 +246,8 @@ def build_case_sample(scheme="ark23"):
     """Horizontal sub-sample of the benchmark workload: 4x4 of the 16x16
     element columns at full height, identical spacing, physics and dt."""
     import numpy as np
-    import problems as P
+    load_pkg()
+    from atum_b200 import workloads as P
     import atum_b200 as A
     full = build_case(scheme=scheme)
     L = 10e3
@@ -433,12 +442,8 @@ def run_ours(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64-state/f32-flux",
         "data": "synthetic",
-        "config": {"workload": "3-D Euler-gravity rising bubble, 16^3 hexahedra, N=4 (2,560,000 DOFs), EC volume + "
-                               "Rusanov surface flux, " + scheme_label(scheme),
-                   "dofs": dofs, "stages_per_step": stages, "precision": args.precision,
-                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                   "l2": "working set ~0.21 GB > 126 MB L2 (no flush)",
-                   "elements_per_cta": tuned},
+        "config": workload_config(scheme, args.precision),
+        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU", "elements_per_cta": tuned,
         "e2e": {"value": e2e, "unit": "DOF-stage/s", "h2d_bytes_per_step": dofs * 8, "d2h_bytes_per_step": dofs * 8,
                 "steps": ke},
         "gpu_launches": int(n1.value - n0.value),
@@ -463,12 +468,60 @@ def run_ours(args):
         "kernels": prof,
         "clocks": clk.summary(),
     }
+    if world == 1 and args.precision == "fp64" and not args.no_precision_pair:
+        line["fp32flux"] = precision_pair(A, args, scheme, value)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(scheme)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+def precision_pair(A, args, scheme, value_fp64):
+    """The FP32-flux / FP64-state form on the same inputs: its throughput
+    (timed like the headline, inputs resident), and its error after
+    ``args.steps`` steps from the same initial state against the FP64 path --
+    relative L2 (MJ-weighted) and L-infinity per component -- plus the mass
+    drift of both forms (the box is closed: periodic sides, walls at top and
+    bottom)."""
+    import numpy as np
+    import torch
+
+    stream = torch.cuda.current_stream()
+    c64 = build_case("fp64", scheme=scheme)
+    c32 = build_case("fp32flux", scheme=scheme)
+    q = torch.as_tensor(c32.q0, device="cuda").contiguous()
+    A.batch.autotune(c32.dg, q)
+    if scheme == "ark23":
+        A.batch.autotune(c32.lindg, q)
+    s32 = make_solver(A, c32, q, scheme)
+    s32.step(q, args.warmup)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s32.step(q, args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    v32 = c32.q0.size * SCHEME_STAGES[scheme] * args.steps / (ms * 1e-3)
+    # accuracy: both forms from the same initial state, the same steps
+    qa = torch.as_tensor(c64.q0, device="cuda").contiguous()
+    qb = torch.as_tensor(c32.q0, device="cuda").contiguous()
+    make_solver(A, c64, qa, scheme).step(qa, args.steps)
+    make_solver(A, c32, qb, scheme).step(qb, args.steps)
+    torch.cuda.synchronize()
+    diff = (qb - qa).contiguous()
+    rel_l2 = A.weightednorm(c64.dg, diff) / A.weightednorm(c64.dg, qa)
+    ha, hb, h0 = qa.cpu().numpy(), qb.cpu().numpy(), c64.q0
+    linf = [float(np.max(np.abs(hb[c] - ha[c])) / np.max(np.abs(ha[c]))) for c in range(ha.shape[0])]
+    mj = c64.dg.MJ
+    m0 = float(np.sum(mj * h0[0]))
+    return {"value": v32, "unit": "DOF-stage/s", "ms_per_step": ms / args.steps, "steps": args.steps,
+            "speedup_vs_fp64": v32 / value_fp64, "rel_l2_vs_fp64": rel_l2, "rel_linf_vs_fp64_per_component": linf,
+            "steps_compared": args.steps,
+            "mass_drift_fp64": abs(float(np.sum(mj * ha[0])) - m0) / abs(m0),
+            "mass_drift_fp32flux": abs(float(np.sum(mj * hb[0])) - m0) / abs(m0)}
 
 
 PROFILE_TEND = "profiles/tendency_eg3_ec_nq5_bubble16.md"
@@ -492,7 +545,8 @@ def run_serve(args):
     dist, rank, world = dist_init()
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     A = load_pkg()
-    import problems as P
+    load_pkg()
+    from atum_b200 import workloads as P
 
     rng = np.random.default_rng(20261203 + rank)
     vortex_K = list(range(16, 129, 16))
@@ -603,7 +657,8 @@ def run_c5(args):
     A = load_pkg()
     from atum_b200 import _lib
     from atum_b200.cell import points_device
-    import problems as P
+    load_pkg()
+    from atum_b200 import workloads as P
 
     Kx, Ky, Kz = args.c5_elements
     N = 7
@@ -784,7 +839,8 @@ def run_swbatch(args):
     dist, rank, world = dist_init()
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     A = load_pkg()
-    import problems as P
+    load_pkg()
+    from atum_b200 import workloads as P
 
     n_inst, K, N = args.instances, 32, 4
     steps = args.steps if args.steps is not None else 500
@@ -921,6 +977,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32flux"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-precision-pair", action="store_true",
+                    help="bubble: skip the FP32-flux run beside the FP64 headline")
     ap.add_argument("--elements-per-cta", type=int, default=0,
                     help="bubble: launch shape of the explicit operator (elements per CTA) instead of autotuning")
     ap.add_argument("--scheme", default="ark23", choices=sorted(SCHEME_STAGES),

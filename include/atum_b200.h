@@ -14,6 +14,12 @@
  * float64 values, node index i + Nq*(j + Nq*k) fastest, element slowest
  * (src/dgsem.jl:251, q[ijk, e]).  Streams are cudaStream_t passed as void*
  * (NULL = the legacy default stream).
+ *
+ * Devices: an operator lives on the CUDA device that was current when it was
+ * created (every buffer it and its solvers allocate is that device's memory).
+ * Every later call on it, or on a solver built from it, must run with that
+ * device current; the library does not switch devices itself.
+ * atb_lsrk54_step_noalloc checks this and returns ATB_ERR_INVALID otherwise.
  */
 #ifndef ATUM_B200_H
 #define ATUM_B200_H
@@ -173,15 +179,19 @@ int atb_op_apply(atb_op* op, double* const* dq, const double* const* q, double t
 /* LSRK54/LSRK144/RLSRK54/RLSRK144/ARK23 constructors -- src/odesolvers.jl:59-67,138-146,284-309.
  * rhs may be NULL for ARK23 (ARK23(nothing, linrhs, ...)); linrhs is NULL for the explicit kinds.
  * For ARK23 the constructor probes linrhs and factors I - dt a_ii L once per distinct
- * vertical column (src/bandedsystem.jl:1-15, src/odesolvers.jl:264-268). */
+ * vertical column (src/bandedsystem.jl:1-15, src/odesolvers.jl:264-268).
+ * dt must be finite and positive, t0 finite (ATB_ERR_INVALID otherwise). */
 int atb_solver_create(int kind, atb_op* rhs, atb_op* linrhs, double dt, double t0, int split_rhs, int paperversion,
                       atb_solver** out);
 int atb_solver_destroy(atb_solver* s);
 /* dostep! repeated nsteps times -- src/odesolvers.jl:47-57,103-136,312-388 */
 int atb_solver_step(atb_solver* s, double* const* q, int nsteps, void* stream);
-/* solve!(q, timeend, solver; adjust_final) -- src/odesolvers.jl:9-26 */
+/* solve!(q, timeend, solver; adjust_final) -- src/odesolvers.jl:9-26.  A step
+ * that would not advance the clock towards timeend (dt <= 0 or below the
+ * clock's resolution) is rejected with ATB_ERR_INVALID instead of looping. */
 int atb_solve(atb_solver* s, double* const* q, double timeend, int adjust_final, int* steps_out, void* stream);
 int atb_solver_get(const atb_solver* s, double* time, double* dt, double* gamma);
+/* dt must be finite and >= 0 (solve! sets dt = timeend - time on its final step) */
 int atb_solver_set_dt(atb_solver* s, double dt);
 /* Checkpoint / resume (no reference counterpart: the reference writes only VTK
  * snapshots, experiment/euler_gravity/risingbubble.jl:81-95): restores the
@@ -249,7 +259,10 @@ int atb_launch_count(long* n);
  * looks up the array's device address for that device (cudaGetSymbolAddress);
  * make that first call before any stream capture.  All calls share the array:
  * calls that overlap on the GPU race on it and must be serialised by the caller;
- * the increment is cleared at the start of each call. */
+ * the increment is cleared at the start of each call.  The call must run with
+ * the operator's creating device current (the array's address differs per
+ * device); otherwise, and for a non-finite dt, it returns ATB_ERR_INVALID.
+ * Only the operator's active elements are stepped and written back. */
 #define ATB_NOALLOC_MAX_DOFS 524288
 int atb_lsrk54_step_noalloc(atb_op* op, double* const* q, double dt, int nsteps, void* stream);
 

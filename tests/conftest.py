@@ -39,4 +39,6 @@ def atb():
 def orc():
     import pyoracle
     pyoracle.build()
+    # element loops only: results do not depend on the thread count
+    pyoracle.set_threads(min(os.cpu_count() or 1, 32))
     return pyoracle

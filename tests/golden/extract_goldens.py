@@ -55,4 +55,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/extract_goldens.py <path to the Atum.jl checkout>")
+    main(sys.argv[1])

@@ -66,3 +66,33 @@ def test_lgl_tables_match_oracle(orc):
         assert np.allclose(c.D @ np.ones(N + 1), 0, atol=1e-13)
         assert np.allclose(c.D @ c.nodes, 1, atol=1e-12)
         assert abs(c.weights.sum() - 2) < 1e-14
+
+
+@pytest.mark.parametrize("dt", [0.0, -1e-3, float("nan"), float("inf")])
+def test_solver_rejects_unusable_dt_without_gpu(dt):
+    """A dt that is not finite and positive would make solve! loop forever;
+    the constructor rejects it before touching the operators or the device."""
+    from atum_b200 import _lib
+    h = C.c_void_p()
+    L = _lib.lib()
+    rc = L.atb_solver_create(0, None, None, dt, 0.0, 1, 0, C.byref(h))
+    assert rc == -1
+    assert b"dt must be finite and positive" in L.atb_last_error()
+    assert not h.value
+
+
+@pytest.mark.parametrize("sflux", ["roe", "matrix", "ec"])
+def test_fp32flux_with_unported_surface_flux_rejected_without_gpu(sflux):
+    """The FP32-flux form has FP32 arithmetic for the central and Rusanov
+    surface fluxes only; other surface fluxes are refused (not silently run in
+    FP64)."""
+    from atum_b200 import _lib, _device
+    flux = {"roe": A.RoeFlux(), "matrix": A.MatrixFlux(), "ec": A.EntropyConservativeFlux()}[sflux]
+    dg = A.DGSEM(law=A.EulerLaw(2), grid=A.brickgrid(A.LobattoCell(3, 3), ([0, 1, 2], [0, 1, 2])),
+                 surface_numericalflux=flux, volume_form=A.FluxDifferencingForm(A.EntropyConservativeFlux()),
+                 precision="fp32flux")
+    d, keep = _device.make_desc(dg)
+    h = C.c_void_p()
+    rc = _lib.lib().atb_op_create(C.byref(d), None, C.byref(h))
+    assert rc == -1
+    assert b"central and Rusanov surface fluxes only" in _lib.lib().atb_last_error()
