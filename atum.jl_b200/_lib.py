@@ -16,7 +16,7 @@ LIBPATH = os.path.join(HERE, "csrc", "libatumb200.so")
 
 ATB_OK = 0
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", -4: "non-finite state",
-          -5: "HBM budget exceeded", -6: "device wait timed out"}
+          -5: "HBM budget exceeded", -6: "device wait timed out", -7: "stage callback failed"}
 
 
 class AtbError(RuntimeError):
@@ -41,6 +41,8 @@ class OpDesc(C.Structure):
 
 PtrArr = C.c_void_p * 5
 _LIB = None
+# int (*)(double ex_time, double im_time, double* const* q_stage, void* user)
+STAGE_CB = C.CFUNCTYPE(C.c_int, C.c_double, C.c_double, C.POINTER(C.c_void_p), C.c_void_p)
 
 # exported entry points and their argtypes (every one returns int status)
 _VP, _DP, _IP = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int)
@@ -83,6 +85,7 @@ SIGNATURES = {
     "atb_profile_read": [C.c_int, C.POINTER(C.c_long), _DP],
     "atb_launch_count": [C.POINTER(C.c_long)],
     "atb_lsrk54_step_noalloc": [_VP, PtrArr, C.c_double, C.c_int, _VP],
+    "atb_solver_set_stage_callback": [_VP, STAGE_CB, _VP],
 }
 
 
@@ -132,6 +135,28 @@ def field_ptrs(t, ns: int) -> PtrArr:
     for s in range(len(comps), 5):
         arr[s] = arr[0]
     return arr
+
+
+class _DeviceBlock:
+    """A device array given by its address, for zero-copy torch views
+    (``__cuda_array_interface__``)."""
+
+    def __init__(self, ptr: int, shape):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f8", "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
+
+
+def device_view(ptrs, ns: int, shape):
+    """Torch view (no copy) of a state held as ``ns`` device component
+    pointers: one (ns, *shape) tensor when the components are consecutive,
+    else a list of component tensors."""
+    import torch
+
+    n = int(np.prod(shape))
+    p = [int(ptrs[c] or 0) for c in range(ns)]
+    if all(p[c] == p[0] + 8 * n * c for c in range(ns)):
+        return torch.as_tensor(_DeviceBlock(p[0], (ns,) + tuple(shape)), device="cuda")
+    return [torch.as_tensor(_DeviceBlock(p[c], tuple(shape)), device="cuda") for c in range(ns)]
 
 
 def stream_ptr(stream=None):

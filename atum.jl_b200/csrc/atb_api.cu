@@ -449,10 +449,6 @@ int op_create_impl(const atb_op_desc* descs, int n, const double* const* aux_hos
     return fail(ATB_ERR_INVALID,
                 "the FP32-flux form exists for the flux-differencing volume term with the entropy-conservative "
                 "flux (Euler, Euler-gravity, shallow water) or the Kennedy-Gruber flux (Euler, Euler-gravity)");
-  if (d->precision == ATB_PREC_FP32FLUX && d->surface_flux != ATB_FLUX_CENTRAL && d->surface_flux != ATB_FLUX_RUSANOV)
-    return fail(ATB_ERR_INVALID,
-                "the FP32-flux form has FP32 arithmetic for the central and Rusanov surface fluxes only; "
-                "use precision FP64 with surface flux %d", d->surface_flux);
   tend_launch_fn fn = nullptr;
   red_launch_fn rf = nullptr;
   // a compile-time node-count specialisation when one exists, else the
@@ -708,12 +704,13 @@ extern "C" int atb_op_place_instance(atb_op* op, int first_element, const atb_op
   CK(cudaMemcpyAsync(op->d_nbr + (size_t)first_element * 6, nbr, (size_t)Ki * 6 * sizeof(int),
                      cudaMemcpyHostToDevice, st));
   CK(cudaEventRecord(op->geo_ev[gi], st));
-  // aux: a pageable source is staged before the call returns; a page-locked
-  // one is read by the copy engine later and must outlive the copies
+  // aux from host or device memory (unified addressing picks the direction):
+  // a pageable host source is staged before the call returns; a page-locked
+  // or device one is read later and must outlive the copies
   const size_t n = (size_t)Ki * op->Np;
   for (int k = 0; k < op->naux; ++k)
     CK(cudaMemcpyAsync(op->d_aux + (size_t)k * op->stride() + (size_t)first_element * op->Np, aux_host + k * n,
-                       n * sizeof(double), cudaMemcpyHostToDevice, st));
+                       n * sizeof(double), cudaMemcpyDefault, st));
   return ATB_OK;
 }
 
@@ -921,6 +918,9 @@ struct atb_solver {
   // the solver (atb_solver_set_instance_dt) or by the caller
   double* d_dte = nullptr;
   bool own_dte = false;
+  // after_stage (src/odesolvers.jl:10-11,23): host callback between stages
+  atb_stage_callback stage_cb = nullptr;
+  void* stage_user = nullptr;
 };
 
 namespace {
@@ -1093,7 +1093,42 @@ int build_band(atb_solver* s, cudaStream_t st) {
 }
 
 // ------------------------------------------------------------ one step
+// after_stage: the stage's launches are enqueued on st; the callback runs on
+// the host and orders its own device work on st (or synchronises)
+int call_stage(atb_solver* s, double ex_time, double im_time, double* const* qs) {
+  double* p[5];
+  for (int c = 0; c < 5; ++c) p[c] = qs[c < s->ns ? c : 0];
+  const int r = s->stage_cb(ex_time, im_time, p, s->stage_user);
+  if (r != 0) return fail(ATB_ERR_CALLBACK, "stage callback returned %d", r);
+  return ATB_OK;
+}
+
+// LSRK stages with a stage callback: the stage kernel writes the new state to
+// qB and it is copied back into q before the callback, so the callback always
+// sees (and may change) the caller's q, and the next stage starts from it.
+// The arithmetic is that of lsrk_steps.
+int lsrk_steps_cb(atb_solver* s, double* const* q, int nsteps, cudaStream_t st) {
+  atb_op* op = s->rhs;
+  double *dq[5], *qb[5], *cur[5];
+  field_ptrs(s->dq, s->ns, s->stride, dq);
+  field_ptrs(s->qB, s->ns, s->stride, qb);
+  for (int k = 0; k < 5; ++k) cur[k] = q[k < s->ns ? k : 0];
+  for (int n = 0; n < nsteps; ++n) {
+    for (size_t i = 0; i < s->rka.size(); ++i) {
+      int rc = s->d_dte ? run_tendency(op, EPI_LSRK, cur, dq, qb, s->rka[i], s->rkb[i], st, s->d_dte)
+                        : run_tendency(op, EPI_LSRK, cur, dq, qb, s->rka[i], s->rkb[i] * s->dt, st);
+      if (rc) return rc;
+      if ((rc = copy_field(q, qb, s->ns, (size_t)op->K_active * op->Np, st))) return rc;
+      const double t = s->time + s->rkc[i] * s->dt;
+      if ((rc = call_stage(s, t, t, q))) return rc;
+    }
+    s->time += s->dt;
+  }
+  return ATB_OK;
+}
+
 int lsrk_steps(atb_solver* s, double* const* q, int nsteps, cudaStream_t st) {
+  if (s->stage_cb) return lsrk_steps_cb(s, q, nsteps, st);
   atb_op* op = s->rhs;
   double *dq[5], *qb[5], *cur[5], *oth[5];
   field_ptrs(s->dq, s->ns, s->stride, dq);
@@ -1136,9 +1171,15 @@ int rlsrk_step(atb_solver* s, double* const* q, cudaStream_t st) {
     A.n = s->stride;
     A.c = s->rkb[i] * s->dt;
     for (int c = 0; c < 5; ++c) { A.x[c] = q[c < s->ns ? c : 0]; A.y[c] = dq[c]; A.out[c] = q[c < s->ns ? c : 0]; }
-    ProfScope ps(ATB_PROF_COMBINE, st);
-    launch_axpy(A, st);
+    {
+      ProfScope ps(ATB_PROF_COMBINE, st);
+      launch_axpy(A, st);
+    }
     if ((rc = check_launch("axpy"))) return rc;
+    if (s->stage_cb) {
+      const double t = s->time + s->rkc[i] * s->dt;
+      if ((rc = call_stage(s, t, t, q))) return rc;
+    }
   }
   // k = q - q0
   {
@@ -1237,11 +1278,13 @@ int run_fused(atb_solver* s, double* const* Q, const ArkAcc& ark, cudaStream_t s
   int E = op->E;
   int pf = 0;
   for (int j = 0; j < 3; ++j) pf += (ark.acc[j][0] && ark.accin[j][0]) ? 1 : 0;
+  // the compact layout of the Nq-specialised kernels (atb_tendency.cuh)
+  const bool cmp = op->Nq >= 3 && op->Nq <= 8 && fused_compact_fits(op->Nq, op->dim, op->ns, op->npre, op->npv);
   auto bytes = [&](int e) {
-    return tend_smem_bytes(op->ns, op->npre, naux, op->dim, op->Nq, op->Np, op->Nfp, e, op->npv, true, pf);
+    return tend_smem_bytes(op->ns, op->npre, naux, op->dim, op->Nq, op->Np, op->Nfp, e, op->npv, true, pf, cmp);
   };
   // fused kernels are compiled for fused_max_threads per CTA
-  const int maxthr = fused_max_threads(op->Nq);
+  const int maxthr = fused_max_threads(op->Nq, cmp);
   while (E > 1 && (cta_threads(E, op->Np) > maxthr || bytes(E) > 100 * 1024)) --E;
   if (cta_threads(E, op->Np) > maxthr) return fail(ATB_ERR_INVALID, "element too large for the fused ARK stage kernel");
   if (pf && bytes(E) > 227 * 1024) {
@@ -1343,12 +1386,16 @@ int ark_step_accumulated(atb_solver* s, double* const* q, cudaStream_t st) {
   set(a, 0, R2, R2, s->exa[2][1], s->ima[2][1]);
   set(a, 1, F, F, s->exb[1], s->imb[1]);
   if ((rc = stage(R1))) return rc;
+  if (s->stage_cb && (rc = call_stage(s, s->time + s->exc[1] * s->dt, s->time + s->imc[1] * s->dt, R1))) return rc;
   // stage 3 and the update of q
   if ((rc = solve(R2, R2))) return rc;
   acc_clear(a);
   a.adt = s->dt;
   set(a, 0, qq, F, s->exb[2], s->imb[2]);
   if ((rc = stage(R2))) return rc;
+  // (the final update of q is accumulated by this stage's launch, so a
+  // callback that looks at q here already sees the step's result)
+  if (s->stage_cb && (rc = call_stage(s, s->time + s->exc[2] * s->dt, s->time + s->imc[2] * s->dt, R2))) return rc;
   s->time += s->dt;
   return ATB_OK;
 }
@@ -1425,6 +1472,9 @@ int ark_step(atb_solver* s, double* const* q, cudaStream_t st) {
       if ((rc = check_launch("lincomb"))) return rc;
     }
     if ((rc = eval(i))) return rc;
+    if (s->stage_cb &&
+        (rc = call_stage(s, s->time + s->exc[i] * s->dt, s->time + s->imc[i] * s->dt, Q[i])))
+      return rc;
   }
   LinComb C{};
   C.ns = ns;
@@ -1611,7 +1661,7 @@ int fusion_check(atb_solver* s, cudaStream_t st) {
   if (R->K != L->K || R->Np != L->Np || R->stacked != L->stacked) return ATB_OK;
   const int na = R->dim + 3;
   if (R->naux < na || L->naux < na) return ATB_OK;
-  tend_launch_fn f = pick_launcher_fused(R->dim, R->vk, R->Nq);
+  tend_launch_fn f = pick_launcher_fused(R->dim, R->vk, R->Nq, R->sflux, L->sflux);
   if (!f) return ATB_OK;
   unsigned long long* d_cnt = nullptr;
   int rc;
@@ -1661,6 +1711,13 @@ extern "C" int atb_solver_set_instance_dt(atb_solver* s, const double* dt_host) 
   if (!s->d_dte && (rc = dalloc(&s->d_dte, (size_t)op->K))) return rc;
   s->own_dte = true;
   CK(cudaMemcpy(s->d_dte, dte.data(), dte.size() * sizeof(double), cudaMemcpyHostToDevice));
+  return ATB_OK;
+}
+
+extern "C" int atb_solver_set_stage_callback(atb_solver* s, atb_stage_callback cb, void* user) {
+  if (!s) return fail(ATB_ERR_INVALID, "null solver");
+  s->stage_cb = cb;
+  s->stage_user = cb ? user : nullptr;
   return ATB_OK;
 }
 

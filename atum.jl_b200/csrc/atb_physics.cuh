@@ -428,13 +428,314 @@ __device__ __forceinline__ double flux_ws_recip32(const LawP& L, int d, const do
   }
 }
 
-// Central / Rusanov surface flux in the FP32-flux form: the two sides' fluxes
-// from flux_ws_recip32, averaged in FP64; the dissipation is the FP64 jump
-// times an FP32 wave speed.  Other surface fluxes keep their FP64 form.
+// ------------------------------------------------ FP32-flux two-point fluxes
+// F(u) = atanh(sqrt u) / sqrt u = sum_k u^k / (2k+1) and G = 1 / F, eight
+// terms each: below u = 1e-2 the truncation is under 1e-17 relative, so the
+// series branch is as accurate as the logarithm it replaces there
+template <class T> __device__ __forceinline__ T series_F(T u) {
+  return T(1) + u * (T(1) / T(3) + u * (T(1) / T(5) + u * (T(1) / T(7) + u * (T(1) / T(9) +
+         u * (T(1) / T(11) + u * (T(1) / T(13) + u * (T(1) / T(15))))))));
+}
+template <class T> __device__ __forceinline__ T series_G(T u) {
+  return T(1) - u * (T(1) / T(3) + u * (T(4) / T(45) + u * (T(44) / T(945) + u * (T(428) / T(14175) +
+         u * (T(10196) / T(467775) + u * (T(10719068) / T(638512875) + u * (T(25865068) / T(1915538625))))))));
+}
+
+// EC flux, row d, FP32-flux precision form.  Inputs: FP64 rho, p, b and the
+// geopotential; FP32 velocities and |u|^2.  The pressure-like term is the
+// FP64 average of the two pressures plus a second-order FP32 correction,
+//   rho_avg / (2 b_avg) = p_avg - (p1 - p2)(b2 - b1) / (2 (b1 + b2)),
+// and the logarithmic mean of rho is the FP64 average minus a small FP32
+// series correction, so the hydrostatic balance between the pressure and
+// gravity terms is carried in FP64 while every division, logarithm and
+// advective product is FP32.  Returns FP64 row values and b_avg * rho_log.
+template <int LAW, int DIM>
+__device__ __forceinline__ void ec_vol32(float igm1, int d, double r1, double p1, double b1, const float* u1,
+                                         float uu1, double Phi1, double r2, double p2, double b2,
+                                         const float* u2, float uu2, double Phi2, double* f, double* xtra) {
+  const double rho_avg = (r1 + r2) * 0.5, p_avg = (p1 + p2) * 0.5, b_avg = (b1 + b2) * 0.5;
+  const float rs = (float)(r1 + r2), rd = (float)(r1 - r2);
+  const float bs = (float)(b1 + b2), bd = (float)(b1 - b2);
+  const float fr = rd / rs, fb = bd / bs;
+  const float ur = fr * fr, ub = fb * fb;
+  double rho_log;
+  float cterm;
+  if (ur < 1e-2f && ub < 1e-2f) {
+    // 1 - G(u) = u/3 + 4u^2/45 + 44u^3/945 + ... (the terms of series_G)
+    const float cr = ur * (1.f / 3.f + ur * (4.f / 45.f + ur * (44.f / 945.f + ur * (428.f / 14175.f +
+                     ur * (10196.f / 467775.f + ur * (10719068.f / 638512875.f + ur * (25865068.f / 1915538625.f)))))));
+    rho_log = rho_avg - rho_avg * (double)cr;
+    cterm = series_F(ub) * igm1 / bs;  // 1 / (2 (gamma-1) b_log)
+  } else {
+    rho_log = logavg_fast(r1, r2);
+    const float b_log = (ub < 1e-2f) ? 0.5f * bs * series_G(ub) : bd / logf((float)b1 / (float)b2);
+    cterm = 0.5f * igm1 / b_log;
+  }
+  const double corr = (double)((float)(p1 - p2) * (float)(b2 - b1) / (2.f * bs));
+  const double pc = p_avg - corr;
+  float ua[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) ua[c] = 0.5f * (u1[c] + u2[c]);
+  const float rl = (float)rho_log;
+  const float ud = ua[d];
+  const float frd = ud * rl;
+  f[0] = (double)frd;
+  float mu = 0.f;
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    const float m = ud * (ua[c] * rl);
+    f[1 + c] = (double)m;
+    mu += m * ua[c];
+  }
+  f[1 + d] += pc;
+  mu += (float)pc * ud;
+  float c1 = cterm - 0.25f * (uu1 + uu2);
+  if (LAW == LAW_EG) c1 += (float)((Phi1 + Phi2) * 0.5);
+  f[DIM + 1] = (double)(c1 * frd + mu);
+  *xtra = b_avg * rho_log;
+}
+
+// shallow-water EC flux, row d, FP32-flux form: the pressure term
+// g (rho_avg^2 - rho2_avg/2) = g rho1 rho2 / 2 stays FP64, advective products
+// are FP32
+template <int DIM>
+__device__ __forceinline__ void sw_vol32(double grav, int d, const double* q1, const float* P1, const double* q2,
+                                         const float* P2, double* f) {
+  const double md = 0.5 * (q1[1 + d] + q2[1 + d]);
+  const float mdf = (float)md;
+  f[0] = md;
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) f[1 + c] = (double)(mdf * (0.5f * (P1[c] + P2[c])));
+  f[1 + d] += grav * q1[0] * q2[0] * 0.5;
+  f[DIM + 1] = (double)(mdf * (0.5f * (P1[DIM] + P2[DIM])));
+}
+
+// Kennedy-Gruber flux, row d, FP32-flux precision form: the density and
+// pressure averages -- the pressure term balances the FP64 gravity fluctuation
+// of a hydrostatic state -- stay FP64; velocities, the specific energy and the
+// advective products are FP32.
+template <int DIM>
+__device__ __forceinline__ void kg_vol32(int d, double r1, double p1, const float* u1, float e1, double r2, double p2,
+                                         const float* u2, float e2, double* f) {
+  const double rho_avg = (r1 + r2) * 0.5, p_avg = (p1 + p2) * 0.5;
+  const float rf = (float)rho_avg;
+  const float ud = 0.5f * (u1[d] + u2[d]);
+  f[0] = (double)(ud * rf);
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) f[1 + c] = (double)(ud * ((0.5f * (u1[c] + u2[c])) * rf));
+  f[1 + d] = f[1 + d] + p_avg;
+  const float e_avg = 0.5f * (e1 + e2);
+  f[DIM + 1] = (double)(ud * (rf * e_avg)) + (double)ud * p_avg;
+}
+
+// Per-side values of the FP32-flux two-point fluxes, as the volume kernel
+// stages them: FP64 pressure and b = rho / (2 p), FP32 velocity, |u|^2 and
+// specific energy.
+template <int DIM>
+__device__ __forceinline__ void pre32(double gamma, const double* q, double Phi, double* p, double* b, float* u,
+                                      float* uu, float* e) {
+  const double rinv = 1.0 / q[0];
+  const double ke = 0.5 * dot<DIM>(q + 1, q + 1) * rinv;
+  *p = (gamma - 1.0) * (q[DIM + 1] - ke - q[0] * Phi);
+  *b = 0.5 / (*p * rinv);
+  const float rinvf = (float)rinv;
+  float s = 0.f;
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    u[c] = (float)q[1 + c] * rinvf;
+    s += u[c] * u[c];
+  }
+  *uu = s;
+  *e = (float)q[DIM + 1] * rinvf;
+}
+
+// Roe dissipation (src/balancelaws/euler.jl:91-138, euler_gravity.jl:149-198;
+// src/balancelaws/shallow_water.jl:68-110) in FP32 from FP64 jumps of the
+// density, pressure (or height) and velocities, which vanish exactly where
+// the state is continuous -- at rest the dissipation stays exactly zero.
+// Returns the dissipation vector (the flux is central - it).
+template <int LAW, int DIM>
+__device__ __forceinline__ void roe_diss32(const LawP& L, int d, double sgn, const double* qm, const double* am,
+                                           const double* qp, float* fpv) {
+  float n[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) n[c] = (c == d) ? (float)sgn : 0.f;
+  const float rm = (float)qm[0], rp = (float)qp[0];
+  const float rim = 1.f / rm, rip = 1.f / rp;
+  float um[DIM], up[DIM], u[DIM], du[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) { um[c] = (float)qm[1 + c] * rim; up[c] = (float)qp[1 + c] * rip; }
+  const float srm = sqrtf(rm), srp = sqrtf(rp);
+  const float rho = sqrtf(rm * rp);
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) { u[c] = roe_avg(srm, srp, um[c], up[c]); du[c] = up[c] - um[c]; }
+  const float drho = (float)(qp[0] - qm[0]);
+  float c, dp, hm = 0.f, hp = 0.f, thm = 0.f, thp = 0.f;
+  if constexpr (LAW == LAW_SW) {
+    const double pm = L.grav * (qm[0] * qm[0]) / 2.0, pp = L.grav * (qp[0] * qp[0]) / 2.0;
+    dp = (float)(pp - pm);
+    thm = (float)qm[DIM + 1] * rim;
+    thp = (float)qp[DIM + 1] * rip;
+    c = roe_avg(srm, srp, sqrtf((float)L.grav * rm), sqrtf((float)L.grav * rp));
+  } else {
+    const double Phi = (LAW == LAW_EG) ? am[0] : 0.0;
+    const double pm = pressure_eg<DIM>(L.gamma, qm, Phi), pp = pressure_eg<DIM>(L.gamma, qp, Phi);
+    dp = (float)(pp - pm);
+    const float g = (float)L.gamma;
+    hm = ((float)qm[DIM + 1] + (float)pm) * rim;
+    hp = ((float)qp[DIM + 1] + (float)pp) * rip;
+    c = roe_avg(srm, srp, sqrtf(g * (float)pm * rim), sqrtf(g * (float)pp * rip));
+  }
+  const float un = dot<DIM>(u, n), dun = dot<DIM>(du, n);
+  const float cm2 = 1.f / (c * c);
+  const float w1 = fabsf(un - c) * (dp - rho * c * dun) * cm2 / 2.f;
+  const float w2 = fabsf(un + c) * (dp + rho * c * dun) * cm2 / 2.f;
+  const float w3 = fabsf(un) * (drho - dp * cm2);
+  const float w4 = fabsf(un) * rho;
+  fpv[0] = (w1 + w2 + w3) / 2.f;
+#pragma unroll
+  for (int k = 0; k < DIM; ++k)
+    fpv[1 + k] = (w1 * (u[k] - c * n[k]) + w2 * (u[k] + c * n[k]) + w3 * u[k] + w4 * (du[k] - dun * n[k])) / 2.f;
+  if constexpr (LAW == LAW_SW) {
+    const float th = roe_avg(srm, srp, thm, thp);
+    const float w5 = fabsf(un) * ((float)(qp[DIM + 1] - qm[DIM + 1]) - th * dp * cm2);
+    fpv[DIM + 1] = ((w1 + w2) * th + w5) / 2.f;
+  } else {
+    const float h = roe_avg(srm, srp, hm, hp);
+    float ke = w3 * dot<DIM>(u, u) / 2.f;
+    if (LAW == LAW_EG) ke = w3 * (dot<DIM>(u, u) / 2.f + (float)am[0]);
+    fpv[DIM + 1] = (w1 * (h - c * un) + w2 * (h + c * un) + ke + w4 * (dot<DIM>(u, du) - un * dun)) / 2.f;
+  }
+}
+
+// Matrix dissipation (src/balancelaws/euler.jl:198-256, euler_gravity.jl:271-
+// 332, including the reference's u2_bar quirk of norms at :219) in FP32 from
+// the FP64 jump of the entropy variables.  Returns D (the flux is EC - D/2).
+template <int LAW, int DIM>
+__device__ __forceinline__ void matrix_diss32(const LawP& L, int d, double sgn, const double* qm, const double* am,
+                                              const double* qp, const double* ap, double bm64, double bp64,
+                                              const float* um, float uum, const float* up, float uup, float* Dm) {
+  constexpr int NS = NSt<LAW, DIM>::v;
+  const float g = (float)L.gamma;
+  float n[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) n[c] = (c == d) ? (float)sgn : 0.f;
+  const float Phi_avg = (LAW == LAW_EG) ? (float)((am[0] + ap[0]) / 2.0) : 0.f;
+  const float rm = (float)qm[0], rp = (float)qp[0], bm = (float)bm64, bp = (float)bp64;
+  const float rho_log = logavg(rm, rp);
+  const float b_log = logavg(bm, bp);
+  float ua[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) ua[c] = (um[c] + up[c]) / 2.f;
+  const float p_avg = ((rm + rp) / 2.f) / (2.f * ((bm + bp) / 2.f));
+  const float u2_bar = 2.f * sqrtf(dot<DIM>(ua, ua)) - (sqrtf(uum) + sqrtf(uup)) / 2.f;
+  float h_bar = g / (2.f * b_log * (g - 1.f)) + u2_bar / 2.f;
+  if (LAW == LAW_EG) h_bar += Phi_avg;
+  const float c_bar = sqrtf(g * p_avg / rho_log);
+  float umc[DIM], upc[DIM], ut[DIM];
+  const float un = dot<DIM>(ua, n);
+#pragma unroll
+  for (int k = 0; k < DIM; ++k) {
+    umc[k] = ua[k] - c_bar * n[k];
+    upc[k] = ua[k] + c_bar * n[k];
+    ut[k] = ua[k] - un * n[k];
+  }
+  double vm[NS], vp[NS];
+  entropyvars<LAW, DIM>(L, qm, am, vm);
+  entropyvars<LAW, DIM>(L, qp, ap, vp);
+  float dv[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) dv[s] = (float)(vp[s] - vm[s]);
+  const float l1 = fabsf(un - c_bar) * rho_log / (2.f * g);
+  const float l2 = fabsf(un) * rho_log * (g - 1.f) / g;
+  const float l3 = fabsf(un + c_bar) * rho_log / (2.f * g);
+  const float l4 = fabsf(un) * p_avg;
+  float k2 = u2_bar / 2.f;
+  if (LAW == LAW_EG) k2 += Phi_avg;
+  const float w1 = l1 * (dv[0] + dot<DIM>(umc, dv + 1) + (h_bar - c_bar * un) * dv[DIM + 1]);
+  const float w2 = l2 * (dv[0] + dot<DIM>(ua, dv + 1) + k2 * dv[DIM + 1]);
+  const float w3 = l3 * (dv[0] + dot<DIM>(upc, dv + 1) + (h_bar + c_bar * un) * dv[DIM + 1]);
+  const float ndv = dot<DIM>(n, dv + 1);
+  Dm[0] = w1 + w2 + w3;
+#pragma unroll
+  for (int k = 0; k < DIM; ++k)
+    Dm[1 + k] = w1 * umc[k] + w2 * ua[k] + w3 * upc[k] + l4 * (dv[1 + k] - ndv * n[k] + dv[DIM + 1] * ut[k]);
+  Dm[DIM + 1] = w1 * (h_bar - c_bar * un) + w2 * k2 + w3 * (h_bar + c_bar * un) +
+                l4 * (dot<DIM>(ut, dv + 1) + dv[DIM + 1] * (dot<DIM>(ua, ua) - un * un));
+}
+
+// Surface fluxes in the FP32-flux form.  Central / Rusanov: the two sides'
+// fluxes from flux_ws_recip32, averaged in FP64; the dissipation is the FP64
+// jump times an FP32 wave speed.  EC / KG: the volume term's FP32-flux
+// two-point fluxes (ec_vol32 / kg_vol32 / sw_vol32) of the two face states.
+// Roe: the central part as for Rusanov, the upwind dissipation from
+// roe_diss32.  Matrix: the FP32-flux EC flux minus half of matrix_diss32.
 template <int LAW, int DIM>
 __device__ __forceinline__ bool surface_flux32(const LawP& L, int kind, int d, double sgn, const double* qm,
                                                const double* am, const double* qp, const double* ap, double* nf) {
   constexpr int NS = NSt<LAW, DIM>::v;
+  if constexpr (LAW == LAW_EULER || LAW == LAW_EG) {
+    if (kind == F_EC || kind == F_KG || kind == F_MATRIX) {
+      const double Phim = (LAW == LAW_EG) ? am[0] : 0.0, Phip = (LAW == LAW_EG) ? ap[0] : 0.0;
+      double pm, pp, bm, bp;
+      float um[DIM], up[DIM], uum, uup, em, ep;
+      pre32<DIM>(L.gamma, qm, Phim, &pm, &bm, um, &uum, &em);
+      pre32<DIM>(L.gamma, qp, Phip, &pp, &bp, up, &uup, &ep);
+      double f[NS + 1];
+      if (kind == F_KG) {
+        kg_vol32<DIM>(d, qm[0], pm, um, em, qp[0], pp, up, ep, f);
+      } else {
+        ec_vol32<LAW, DIM>((float)(1.0 / (L.gamma - 1.0)), d, qm[0], pm, bm, um, uum, Phim, qp[0], pp, bp, up,
+                           uup, Phip, f, f + NS);
+      }
+#pragma unroll
+      for (int s = 0; s < NS; ++s) nf[s] = f[s] * sgn;
+      if (kind == F_MATRIX) {
+        float Dm[NS];
+        matrix_diss32<LAW, DIM>(L, d, sgn, qm, am, qp, ap, bm, bp, um, uum, up, uup, Dm);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) nf[s] = nf[s] - (double)(Dm[s] / 2.f);
+      }
+      return true;
+    }
+  }
+  if constexpr (LAW == LAW_SW) {
+    if (kind == F_EC) {
+      float Pm[DIM + 1], Pp[DIM + 1];
+      const float him = 1.f / (float)qm[0], hip = 1.f / (float)qp[0];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) { Pm[c] = (float)qm[1 + c] * him; Pp[c] = (float)qp[1 + c] * hip; }
+      Pm[DIM] = (float)qm[DIM + 1] * him;
+      Pp[DIM] = (float)qp[DIM + 1] * hip;
+      double f[NS];
+      sw_vol32<DIM>(L.grav, d, qm, Pm, qp, Pp, f);
+#pragma unroll
+      for (int s = 0; s < NS; ++s) nf[s] = f[s] * sgn;
+      if (L.swtopo) {  // non-conservative surface term g h- (b+ - b-)/2 n, FP64 (balance)
+        const double t = L.grav * qm[0] * (ap[0] - am[0]) / 2.0;
+        nf[1 + d] = nf[1 + d] + t * sgn;
+      }
+      return true;
+    }
+  }
+  if constexpr (LAW == LAW_EULER || LAW == LAW_EG || LAW == LAW_SW) {
+    if (kind == F_ROE) {
+      double fm[NS], fp[NS];
+      flux_ws_recip32<LAW, DIM>(L, d, qm, am, fm);
+      flux_ws_recip32<LAW, DIM>(L, d, qp, ap, fp);
+      float fpv[NS];
+      roe_diss32<LAW, DIM>(L, d, sgn, qm, am, qp, fpv);
+#pragma unroll
+      for (int s = 0; s < NS; ++s) nf[s] = ((fm[s] + fp[s]) * sgn) / 2.0 - (double)fpv[s];
+      if constexpr (LAW == LAW_SW) {
+        if (L.swtopo) {  // non-conservative surface term g h- (b+ - b-)/2 n, FP64 (balance)
+          const double t = L.grav * qm[0] * (ap[0] - am[0]) / 2.0;
+          nf[1 + d] = nf[1 + d] + t * sgn;
+        }
+      }
+      return true;
+    }
+  }
   if constexpr (LAW == LAW_EULER || LAW == LAW_EG || LAW == LAW_SW) {
     if (kind == F_CENTRAL || kind == F_RUSANOV) {
       double fm[NS], fp[NS];

@@ -116,17 +116,36 @@ template <int LAW, int DIM, int VK> struct NPairVals {
   static constexpr int stride = v | 1;
 };
 
+// cmp: the compact layout of the fused Euler-gravity stage (fused_compact_fits)
 inline size_t tend_smem_bytes(int ns, int npre, int naux, int dim, int Nq, int Np, int Nfp, int E, int npvs,
-                              bool fuse = false, int pf = 0) {
+                              bool fuse = false, int pf = 0, bool cmp = false) {
   const int npl = Nq * (Nq - 1) / 2;
-  size_t per = (size_t)(ns + naux + npre) * Np + (size_t)2 * dim * Nfp * ns;
-  if (npvs > 0) per += (size_t)Nfp * npl * npvs;
-  if (fuse) per += (size_t)ns * Np + (size_t)2 * Nfp * ns;  // linear flux rows, linear face slots
-  per += (size_t)pf * ns * Np;                              // prefetched epilogue inputs
+  size_t per;
+  if (cmp) {
+    per = (size_t)(ns + 3 + npre) * Np + (size_t)Nfp * npl * npvs + (size_t)ns * Np;
+  } else {
+    per = (size_t)(ns + naux + npre) * Np + (size_t)2 * dim * Nfp * ns;
+    if (npvs > 0) per += (size_t)Nfp * npl * npvs;
+    if (fuse) per += (size_t)ns * Np + (size_t)2 * Nfp * ns;  // linear flux rows, linear face slots
+  }
+  per += (size_t)pf * ns * Np;  // prefetched epilogue inputs
   return sizeof(double) * (2 * (size_t)Nq * Nq + 2 + per * E) + 64 * sizeof(int);
 }
 
 __host__ __device__ constexpr int ipow(int b, int e) { return e == 0 ? 1 : b * ipow(b, e - 1); }
+
+// Compact shared-memory layout of the fused Euler-gravity ARK stage: three
+// aux fields per node are staged (Phi, rho_ref, p_ref -- all that the volume
+// term and the face fluxes read of other nodes; grad Phi enters only the
+// linear operator's source, evaluated from registers before the face tasks),
+// the explicit face slots reuse the per-node precomputed values' region, and
+// the parked accumulators, the parked linear source and the linear face slots
+// reuse the pair buffer once the volume term is done.  It applies when those
+// regions are large enough (Nq >= 5 for the FP64 EC flux).
+__host__ __device__ constexpr bool fused_compact_fits(int nq, int dim, int ns, int npre, int npvs) {
+  return nq > 0 && npre * ipow(nq, dim) >= 2 * dim * ipow(nq, dim - 1) * ns &&
+         ipow(nq, dim - 1) * (nq * (nq - 1) / 2) * npvs >= (ns + dim) * ipow(nq, dim) + 2 * ipow(nq, dim - 1) * ns;
+}
 
 // volume-term two-point fluxes on the staged per-node layouts (row d)
 //
@@ -141,18 +160,6 @@ __host__ __device__ constexpr int ipow(int b, int e) { return e == 0 ? 1 : b * i
 // and G = 1/F to the same order (truncation below 1e-17 relative for
 // u < 1e-2).  Otherwise the general form below is used.  A wide series range
 // keeps the pairs of a warp on one branch.
-// F(u) = atanh(sqrt u) / sqrt u = sum_k u^k / (2k+1) and G = 1 / F, eight
-// terms each: below u = 1e-2 the truncation is under 1e-17 relative, so the
-// series branch is as accurate as the logarithm it replaces there
-template <class T> __device__ __forceinline__ T series_F(T u) {
-  return T(1) + u * (T(1) / T(3) + u * (T(1) / T(5) + u * (T(1) / T(7) + u * (T(1) / T(9) +
-         u * (T(1) / T(11) + u * (T(1) / T(13) + u * (T(1) / T(15))))))));
-}
-template <class T> __device__ __forceinline__ T series_G(T u) {
-  return T(1) - u * (T(1) / T(3) + u * (T(4) / T(45) + u * (T(44) / T(945) + u * (T(428) / T(14175) +
-         u * (T(10196) / T(467775) + u * (T(10719068) / T(638512875) + u * (T(25865068) / T(1915538625))))))));
-}
-
 template <int LAW, int DIM, class T>
 __device__ __forceinline__ void ec_vol(T gamma, T igm1, int d, T r1, const T* P1, T Phi1, T r2, const T* P2, T Phi2,
                                        T* f, T* xtra) {
@@ -198,75 +205,6 @@ __device__ __forceinline__ void ec_vol(T gamma, T igm1, int d, T r1, const T* P1
   *xtra = b_avg * rho_log;
 }
 
-// EC flux, row d, FP32-flux precision form.  Inputs: FP64 rho, p, b and the
-// geopotential; FP32 velocities and |u|^2.  The pressure-like term is the
-// FP64 average of the two pressures plus a second-order FP32 correction,
-//   rho_avg / (2 b_avg) = p_avg - (p1 - p2)(b2 - b1) / (2 (b1 + b2)),
-// and the logarithmic mean of rho is the FP64 average minus a small FP32
-// series correction, so the hydrostatic balance between the pressure and
-// gravity terms is carried in FP64 while every division, logarithm and
-// advective product is FP32.  Returns FP64 row values and b_avg * rho_log.
-template <int LAW, int DIM>
-__device__ __forceinline__ void ec_vol32(float igm1, int d, double r1, double p1, double b1, const float* u1,
-                                         float uu1, double Phi1, double r2, double p2, double b2,
-                                         const float* u2, float uu2, double Phi2, double* f, double* xtra) {
-  const double rho_avg = (r1 + r2) * 0.5, p_avg = (p1 + p2) * 0.5, b_avg = (b1 + b2) * 0.5;
-  const float rs = (float)(r1 + r2), rd = (float)(r1 - r2);
-  const float bs = (float)(b1 + b2), bd = (float)(b1 - b2);
-  const float fr = rd / rs, fb = bd / bs;
-  const float ur = fr * fr, ub = fb * fb;
-  double rho_log;
-  float cterm;
-  if (ur < 1e-2f && ub < 1e-2f) {
-    // 1 - G(u) = u/3 + 4u^2/45 + 44u^3/945 + ... (the terms of series_G)
-    const float cr = ur * (1.f / 3.f + ur * (4.f / 45.f + ur * (44.f / 945.f + ur * (428.f / 14175.f +
-                     ur * (10196.f / 467775.f + ur * (10719068.f / 638512875.f + ur * (25865068.f / 1915538625.f)))))));
-    rho_log = rho_avg - rho_avg * (double)cr;
-    cterm = series_F(ub) * igm1 / bs;  // 1 / (2 (gamma-1) b_log)
-  } else {
-    rho_log = logavg_fast(r1, r2);
-    const float b_log = (ub < 1e-2f) ? 0.5f * bs * series_G(ub) : bd / logf((float)b1 / (float)b2);
-    cterm = 0.5f * igm1 / b_log;
-  }
-  const double corr = (double)((float)(p1 - p2) * (float)(b2 - b1) / (2.f * bs));
-  const double pc = p_avg - corr;
-  float ua[DIM];
-#pragma unroll
-  for (int c = 0; c < DIM; ++c) ua[c] = 0.5f * (u1[c] + u2[c]);
-  const float rl = (float)rho_log;
-  const float ud = ua[d];
-  const float frd = ud * rl;
-  f[0] = (double)frd;
-  float mu = 0.f;
-#pragma unroll
-  for (int c = 0; c < DIM; ++c) {
-    const float m = ud * (ua[c] * rl);
-    f[1 + c] = (double)m;
-    mu += m * ua[c];
-  }
-  f[1 + d] += pc;
-  mu += (float)pc * ud;
-  float c1 = cterm - 0.25f * (uu1 + uu2);
-  if (LAW == LAW_EG) c1 += (float)((Phi1 + Phi2) * 0.5);
-  f[DIM + 1] = (double)(c1 * frd + mu);
-  *xtra = b_avg * rho_log;
-}
-
-// shallow-water EC flux, row d, FP32-flux form: the pressure term
-// g (rho_avg^2 - rho2_avg/2) = g rho1 rho2 / 2 stays FP64, advective products
-// are FP32
-template <int DIM>
-__device__ __forceinline__ void sw_vol32(double grav, int d, const double* q1, const float* P1, const double* q2,
-                                         const float* P2, double* f) {
-  const double md = 0.5 * (q1[1 + d] + q2[1 + d]);
-  const float mdf = (float)md;
-  f[0] = md;
-#pragma unroll
-  for (int c = 0; c < DIM; ++c) f[1 + c] = (double)(mdf * (0.5f * (P1[c] + P2[c])));
-  f[1 + d] += grav * q1[0] * q2[0] * 0.5;
-  f[DIM + 1] = (double)(mdf * (0.5f * (P1[DIM] + P2[DIM])));
-}
-
 template <int DIM, class T>
 __device__ __forceinline__ void kg_vol(int d, T r1, const T* P1, T r2, const T* P2, T* f) {
   const T rho_avg = (r1 + r2) / T(2);
@@ -284,31 +222,15 @@ __device__ __forceinline__ void kg_vol(int d, T r1, const T* P1, T r2, const T* 
   f[DIM + 1] = ud * (rho_avg * e_avg + p_avg);
 }
 
-// Kennedy-Gruber flux, row d, FP32-flux precision form: the density and
-// pressure averages -- the pressure term balances the FP64 gravity fluctuation
-// of a hydrostatic state -- stay FP64; velocities, the specific energy and the
-// advective products are FP32.
-template <int DIM>
-__device__ __forceinline__ void kg_vol32(int d, double r1, double p1, const float* u1, float e1, double r2, double p2,
-                                         const float* u2, float e2, double* f) {
-  const double rho_avg = (r1 + r2) * 0.5, p_avg = (p1 + p2) * 0.5;
-  const float rf = (float)rho_avg;
-  const float ud = 0.5f * (u1[d] + u2[d]);
-  f[0] = (double)(ud * rf);
-#pragma unroll
-  for (int c = 0; c < DIM; ++c) f[1 + c] = (double)(ud * ((0.5f * (u1[c] + u2[c])) * rf));
-  f[1 + d] = f[1 + d] + p_avg;
-  const float e_avg = 0.5f * (e1 + e2);
-  f[DIM + 1] = (double)(ud * (rf * e_avg)) + (double)ud * p_avg;
-}
-
 // pair index of nodes a < b on a line of Nq nodes
 __device__ __forceinline__ int pair_index(int a, int b, int Nq) { return a * Nq - a * (a + 1) / 2 + (b - a - 1); }
 
 // one face-node task (face t / Nfp of direction D_, node t % Nfp): gather
 // the neighbour trace (or the boundary state), evaluate the numerical flux and
 // store it lifted into the face's shared-memory slot
-template <int LAW, int DIM, int NAM, int D_, bool F32S = false>
+// CMPA: the staged aux fields are the compact [Phi, rho_ref, p_ref]
+// (components 0, DIM+1, DIM+2; the face fluxes read no others)
+template <int LAW, int DIM, int NAM, int D_, bool F32S = false, bool CMPA = false>
 __device__ __forceinline__ void face_task(const TendArgs& A, const LawP& L, int sflux, int naux, int Nq, int Np,
                                           int Nfp, int e, int t, const double* sq, const double* sa, double* ss,
                                           double gid, double lift_end) {
@@ -323,7 +245,14 @@ __device__ __forceinline__ void face_task(const TendArgs& A, const LawP& L, int 
 #pragma unroll
   for (int s = 0; s < NS; ++s) qm[s] = sq[s * Np + nm];
 #pragma unroll
-  for (int k = 0; k < NAM; ++k) am[k] = (k < naux) ? sa[k * Np + nm] : 0.0;
+  for (int k = 0; k < NAM; ++k) {
+    if constexpr (CMPA) {
+      const int c = (k == 0) ? 0 : (k == DIM + 1) ? 1 : (k == DIM + 2) ? 2 : -1;
+      am[k] = (k < naux && c >= 0) ? sa[c * Np + nm] : 0.0;
+    } else {
+      am[k] = (k < naux) ? sa[k * Np + nm] : 0.0;
+    }
+  }
   // neighbour table entries are relative (neighbour element - e), or a
   // boundary tag offset by NBR_BOUNDARY
   const int nv = __ldg(A.nbr + 6 * e + face);
@@ -354,16 +283,32 @@ __device__ __forceinline__ void face_task(const TendArgs& A, const LawP& L, int 
 // NQ_ > 0: the node count per direction is a compile-time constant (index
 // arithmetic folds, line loops unroll); NQ_ = 0 reads it from the arguments.
 // CTA size limit of the fused kernels: 256 threads unless one element needs
-// more
-__host__ __device__ constexpr int fused_max_threads(int nq) { return (nq == 0 || nq * nq * nq > 256) ? 512 : 256; }
+// more; with the compact layout at Nq = 5 (125 nodes), one element per CTA of
+// 128 threads and five CTAs per SM (43 KB of shared memory each, 96 registers).
+// cmp: the kernel uses the compact layout (fused_compact_fits).
+__host__ __device__ constexpr int fused_max_threads(int nq, bool cmp = false) {
+  return (nq == 0 || nq * nq * nq > 256) ? 512 : (cmp && nq == 5) ? 128 : 256;
+}
+__host__ __device__ constexpr int fused_min_blocks(int nq, bool cmp = false) {
+  return (cmp && nq == 5) ? 5 : 512 / fused_max_threads(nq, cmp);
+}
 
 // Plain launches: up to 512 threads.  Fused launches (which carry the linear
 // operator too): fused_max_threads, with enough resident CTAs requested that
 // the register budget stays at 128 -- measured faster on B200 than the
 // spill-free 156-register allocation, whose lower occupancy costs more.
-template <int LAW, int DIM, int VK, int NQ_, bool FUSE = false>
-__global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 512 / fused_max_threads(NQ_) : 1)
-    tendency_kernel(const TendArgs A) {
+//
+// SF >= 0: the surface flux kind (of the explicit operator and, fused, of the
+// linear one) is a compile-time constant, so the kernel carries one numerical
+// flux instead of all of them; SF = -1 reads it from the arguments.
+template <int LAW, int DIM, int VK, int NQ_, bool FUSE = false, int SF = -1>
+__global__ void __launch_bounds__(
+    FUSE ? fused_max_threads(NQ_, LAW == LAW_EG && fused_compact_fits(NQ_, DIM, NSt<LAW, DIM>::v, NPre<LAW, DIM, VK>::v,
+                                                                        NPairVals<LAW, DIM, VK>::stride))
+         : 512,
+    FUSE ? fused_min_blocks(NQ_, LAW == LAW_EG && fused_compact_fits(NQ_, DIM, NSt<LAW, DIM>::v, NPre<LAW, DIM, VK>::v,
+                                                                       NPairVals<LAW, DIM, VK>::stride))
+         : 1) tendency_kernel(const TendArgs A) {
   constexpr int NS = NSt<LAW, DIM>::v;
   constexpr int NPRE = NPre<LAW, DIM, VK>::v;
   constexpr int NAM = NAuxMax<LAW, DIM>::v;
@@ -375,12 +320,17 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
   constexpr int NPV = PAIRS ? NPairVals<LAW, DIM, VK>::v : 0;
   constexpr int NPVS = PAIRS ? NPairVals<LAW, DIM, VK>::stride : 0;
   constexpr bool CQ = NQ_ > 0;
+  // the fused kernel runs the ARK23 stage epilogue only
+  const int epi = FUSE ? EPI_ARK : A.epi;
+  const int sflux = SF >= 0 ? SF : A.sflux;
+  const int lin_sflux = SF >= 0 ? SF : A.lin_sflux;
   extern __shared__ double sm[];
   const int Nq = CQ ? NQ_ : A.Nq;
   const int Np = CQ ? ipow(NQ_, DIM) : A.Np;
   const int Nfp = CQ ? ipow(NQ_, DIM - 1) : A.Nfp;
   const int naux = A.naux;
   const int npl = Nq * (Nq - 1) / 2;
+  constexpr bool CMP = FUSE && LAW == LAW_EG && fused_compact_fits(NQ_, DIM, NS, NPRE, NPVS);
   const int slot = threadIdx.x / Np;
   const int node = threadIdx.x - slot * Np;
   const int e = blockIdx.x * A.E + slot;
@@ -388,15 +338,21 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
   const int tabn = 2 * Nq * Nq + 2;
   double* sC = sm;            // Cfd
   double* sW = sm + Nq * Nq;  // Cw
-  const size_t slotsz = (size_t)(NS + naux + NPRE) * Np + (size_t)2 * DIM * Nfp * NS + (size_t)Nfp * npl * NPVS +
-                        (FUSE ? (size_t)NS * Np + (size_t)2 * Nfp * NS : 0) + (size_t)A.pf * NS * Np;
+  const int naux_s = CMP ? 3 : naux;  // aux fields staged in shared memory
+  const size_t slotsz =
+      CMP ? (size_t)(NS + 3 + NPRE) * Np + (size_t)Nfp * npl * NPVS + (size_t)NS * Np + (size_t)A.pf * NS * Np
+          : (size_t)(NS + naux + NPRE) * Np + (size_t)2 * DIM * Nfp * NS + (size_t)Nfp * npl * NPVS +
+                (FUSE ? (size_t)NS * Np + (size_t)2 * Nfp * NS : 0) + (size_t)A.pf * NS * Np;
   double* sq = sm + tabn + slot * slotsz;
   double* sa = sq + NS * Np;
-  double* sp = sa + naux * Np;
-  double* ss = sp + NPRE * Np;
-  double* spv = ss + 2 * DIM * Nfp * NS;  // pair values
+  double* sp = sa + naux_s * Np;
+  // compact: the explicit face slots take the precomputed values' region
+  double* ss = CMP ? sp : sp + NPRE * Np;
+  double* spv = CMP ? sp + NPRE * Np : ss + 2 * DIM * Nfp * NS;  // pair values
   double* slf = spv + (size_t)Nfp * npl * NPVS;  // FUSE: linear vertical flux per node
-  double* ssl = slf + NS * Np;                   // FUSE: linear z-face slots
+  // FUSE: linear z-face slots (compact: in the pair buffer, after the parked
+  // accumulators and the parked linear source)
+  double* ssl = CMP ? spv + (size_t)(NS + DIM) * Np : slf + NS * Np;
   // prefetched epilogue inputs: the last A.pf*NS*Np doubles of the slot
   double* spf_in = sq + slotsz - (size_t)A.pf * NS * Np;
   int* spair = (int*)(sm + tabn + A.E * slotsz);
@@ -421,7 +377,7 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
       for (int s = 0; s < NS; ++s) tend_cp_async8(spf_in + (j * NS + s) * Np + node, P[s] + gid);
       ++j;
     };
-    switch (A.epi) {
+    switch (epi) {
       case EPI_ADD: pf5(A.out[0], A.out[1], A.out[2], A.out[3], A.out[4]); break;
       case EPI_LSRK:
         if (A.a != 0.0) pf5(A.out[0], A.out[1], A.out[2], A.out[3], A.out[4]);
@@ -451,7 +407,13 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
     for (int k = 0; k < NAM; ++k)
       if (k < naux) {
         an[k] = __ldg(A.aux + k * A.stride + gid);
-        sa[k * Np + node] = an[k];
+        if constexpr (CMP) {
+          if (k == 0) sa[node] = an[k];
+          if (k == DIM + 1) sa[Np + node] = an[k];
+          if (k == DIM + 2) sa[2 * Np + node] = an[k];
+        } else {
+          sa[k * Np + node] = an[k];
+        }
       }
     if constexpr (VK == VK_EC && LAW == LAW_SW) {
 #pragma unroll
@@ -689,6 +651,20 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
       for (int s = 0; s < NS; ++s) spv[s * Np + node] = T[s];
     }
   }
+  // compact layout: the linear operator's source (it reads grad Phi, which is
+  // not staged) is evaluated now, from registers, exactly as the linear
+  // operator begins -- TL = 0, then its sources -- and parked with T; it only
+  // touches the momentum components
+  if constexpr (CMP) {
+    if (act && ((A.lin_dirs >> (DIM - 1)) & 1)) {
+      double tl[NS];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) tl[s] = 0.0;
+      add_sources<LAW_LEG, DIM>(A.lin_law, true, qn, an, tl);
+#pragma unroll
+      for (int k = 0; k < DIM; ++k) spv[(NS + k) * Np + node] = tl[1 + k];
+    }
+  }
 
   // ------------------------------------------------------------ faces
   // Face-node tasks of all elements of the CTA, spread over all its threads.
@@ -713,23 +689,25 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
       if (tt >= 2 * Nfp || ef >= A.K) continue;
       double* const sqe = sm + tabn + es * slotsz;
       double* const sae = sqe + NS * Np;
-      double* const sse = sae + naux * Np + NPRE * Np;
+      double* const spe = sae + naux_s * Np;
+      double* const sse = CMP ? spe : spe + NPRE * Np;
       if constexpr (FUSE && LAW == LAW_EG) {
         if (dd == DIM) {
           // z faces of the linear operator (face numbers 2*DZ, 2*DZ + 1): the
           // slot pointer is shifted so those faces land in the linear slots
-          double* const ssle = sse + 2 * DIM * Nfp * NS + (size_t)Nfp * npl * NPVS + NS * Np;
-          face_task<LAW_LEG, DIM, NAuxMax<LAW_LEG, DIM>::v, DZ>(
-              A, A.lin_law, A.lin_sflux, naux, Nq, Np, Nfp, ef, 2 * DZ * Nfp + tt, sqe, sae,
+          double* const ssle = CMP ? spe + NPRE * Np + (size_t)(NS + DIM) * Np
+                                   : sse + 2 * DIM * Nfp * NS + (size_t)Nfp * npl * NPVS + NS * Np;
+          face_task<LAW_LEG, DIM, NAuxMax<LAW_LEG, DIM>::v, DZ, false, CMP>(
+              A, A.lin_law, lin_sflux, naux, Nq, Np, Nfp, ef, 2 * DZ * Nfp + tt, sqe, sae,
               ssle - (size_t)2 * DZ * Nfp * NS, __ldg(A.ginv + 3 * ef + DZ), lift_end);
           continue;
         }
       }
       const int t = 2 * dd * Nfp + tt;
       switch (dd) {
-        case 0: face_task<LAW, DIM, NAM, 0, F32S>(A, L, A.sflux, naux_nl, Nq, Np, Nfp, ef, t, sqe, sae, sse, __ldg(A.ginv + 3 * ef), lift_end); break;
-        case 1: if constexpr (DIM > 1) face_task<LAW, DIM, NAM, 1, F32S>(A, L, A.sflux, naux_nl, Nq, Np, Nfp, ef, t, sqe, sae, sse, __ldg(A.ginv + 3 * ef + 1), lift_end); break;
-        default: if constexpr (DIM > 2) face_task<LAW, DIM, NAM, 2, F32S>(A, L, A.sflux, naux_nl, Nq, Np, Nfp, ef, t, sqe, sae, sse, __ldg(A.ginv + 3 * ef + 2), lift_end); break;
+        case 0: face_task<LAW, DIM, NAM, 0, F32S, CMP>(A, L, sflux, naux_nl, Nq, Np, Nfp, ef, t, sqe, sae, sse, __ldg(A.ginv + 3 * ef), lift_end); break;
+        case 1: if constexpr (DIM > 1) face_task<LAW, DIM, NAM, 1, F32S, CMP>(A, L, sflux, naux_nl, Nq, Np, Nfp, ef, t, sqe, sae, sse, __ldg(A.ginv + 3 * ef + 1), lift_end); break;
+        default: if constexpr (DIM > 2) face_task<LAW, DIM, NAM, 2, F32S, CMP>(A, L, sflux, naux_nl, Nq, Np, Nfp, ef, t, sqe, sae, sse, __ldg(A.ginv + 3 * ef + 2), lift_end); break;
       }
     }
   }
@@ -741,9 +719,12 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
       T[s] = spv[s * Np + node];
       qn[s] = sq[s * Np + node];
     }
+    // (compact layout: nothing after this point reads the aux fields)
+    if constexpr (!CMP) {
 #pragma unroll
-    for (int k = 0; k < NAM; ++k)
-      if (k < naux) an[k] = sa[k * Np + node];
+      for (int k = 0; k < NAM; ++k)
+        if (k < naux) an[k] = sa[k * Np + node];
+    }
   }
 #pragma unroll
   for (int d = 0; d < DIM; ++d) {
@@ -763,7 +744,12 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
   for (int s = 0; s < NS; ++s) TL[s] = 0.0;
   if constexpr (FUSE && LAW == LAW_EG) {
     if ((A.lin_dirs >> DZ) & 1) {
-      add_sources<LAW_LEG, DIM>(A.lin_law, true, qn, an, TL);
+      if constexpr (CMP) {
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) TL[1 + k] = spv[(NS + k) * Np + node];
+      } else {
+        add_sources<LAW_LEG, DIM>(A.lin_law, true, qn, an, TL);
+      }
       const int sd = (DZ == 0) ? 1 : (DZ == 1) ? Nq : Nq * Nq;
       const int id = ijk[DZ];
       const int base = node - id * sd;
@@ -791,7 +777,7 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
   if (pfon) asm volatile("cp.async.wait_all;\n" ::: "memory");
   // j-th prefetched field, state s (own node); the same order as issued
   auto pin = [&](int j, int s) { return spf_in[(j * NS + s) * Np + node]; };
-  switch (A.epi) {
+  switch (epi) {
     case EPI_SET:
 #pragma unroll
       for (int s = 0; s < NS; ++s) A.out[s][gid] = T[s];
@@ -849,22 +835,33 @@ __global__ void __launch_bounds__(FUSE ? fused_max_threads(NQ_) : 512, FUSE ? 51
 // launcher signature used by the host dispatch table
 typedef void (*tend_launch_fn)(const TendArgs& A, int grid, int block, size_t smem, cudaStream_t st);
 
-template <int LAW, int DIM, int VK, int NQ_ = 0, bool FUSE = false>
+template <int LAW, int DIM, int VK, int NQ_ = 0, bool FUSE = false, int SF = -1>
 void tend_launch(const TendArgs& A, int grid, int block, size_t smem, cudaStream_t st) {
   static size_t configured = 0;
+  static bool carveout = false;
+  if (FUSE && !carveout) {
+    // the fused stage kernels are occupancy-limited by shared memory: ask for
+    // the largest carveout (a hint; the launch does not depend on it)
+    cudaFuncSetAttribute(tendency_kernel<LAW, DIM, VK, NQ_, FUSE, SF>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         100);
+    cudaGetLastError();
+    carveout = true;
+  }
   if (smem > 48 * 1024 && smem > configured) {
     // on failure the launch below reports the error
-    if (cudaFuncSetAttribute(tendency_kernel<LAW, DIM, VK, NQ_, FUSE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(tendency_kernel<LAW, DIM, VK, NQ_, FUSE, SF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem) == cudaSuccess)
       configured = smem;
   }
-  tendency_kernel<LAW, DIM, VK, NQ_, FUSE><<<grid, block, smem, st>>>(A);
+  tendency_kernel<LAW, DIM, VK, NQ_, FUSE, SF><<<grid, block, smem, st>>>(A);
 }
 
 // Euler-gravity explicit tendency fused with the weak-form linear operator
 // along z (ARK23 stages, split_rhs = false): 3-D, EC / FP32-flux EC volume
 // flux; nullptr when there is no such kernel
-tend_launch_fn pick_launcher_fused(int dim, int vk, int nq);
+// sflux / lin_sflux: the surface fluxes of the two operators (a kernel with
+// the flux kind built in when both are Rusanov)
+tend_launch_fn pick_launcher_fused(int dim, int vk, int nq, int sflux, int lin_sflux);
 
 // generic (runtime Nq) launcher, and the compile-time-Nq specialisations
 // that exist for (law, dim, vk, nq) -- nullptr when there is none

@@ -109,11 +109,45 @@ def solve_(q, timeend: float, solver: Solver, after_step: Optional[Callable] = N
     """``solve!(q, timeend, solver; after_step, after_stage, adjust_final)``.
 
     Returns the number of steps.  ``after_step(step, time, q)`` runs on the
-    host after each step; the stage kernels are fused, so ``after_stage`` is
-    not supported.
+    host after each step.  ``after_stage`` runs on the host between stages, as
+    in the reference (src/odesolvers.jl:54,119,378): LSRK / RLSRK call
+    ``after_stage(stagetime, q)`` after every stage with the caller's ``q``
+    (changes to it carry into the next stage); ARK23 calls
+    ``after_stage((ex_stagetime, im_stagetime), Q)`` after stages 2 and 3 with
+    a zero-copy view ``Q`` of the solver's stage state.  The stage's kernels
+    are enqueued on the stream when the callback runs; torch operations on the
+    same stream are ordered after them.
     """
-    if after_stage is not None:
-        raise NotImplementedError("after_stage callbacks: the stage update is fused into the tendency kernel")
+    if after_stage is None:
+        return _solve(q, timeend, solver, after_step, adjust_final, stream)
+    err = []
+    shape = tuple(q.shape[1:]) if not isinstance(q, (list, tuple)) else tuple(q[0].shape)
+    ark = solver.kind == "ARK23"
+
+    def cb(ex_t, im_t, ptrs, user):
+        try:
+            if ark:
+                after_stage((ex_t, im_t), _lib.device_view(ptrs, solver.ns, shape))
+            else:
+                after_stage(ex_t, q)
+            return 0
+        except BaseException as e:  # re-raised below; a C callback cannot propagate it
+            err.append(e)
+            return 1
+
+    fn = _lib.STAGE_CB(cb)
+    _lib.check(_lib.lib().atb_solver_set_stage_callback(solver.h, fn, None))
+    try:
+        return _solve(q, timeend, solver, after_step, adjust_final, stream)
+    except _lib.AtbError:
+        if err:
+            raise err[0]
+        raise
+    finally:
+        _lib.lib().atb_solver_set_stage_callback(solver.h, _lib.STAGE_CB(), None)
+
+
+def _solve(q, timeend, solver, after_step, adjust_final, stream) -> int:
     if after_step is None:
         steps = C.c_int()
         _lib.check(_lib.lib().atb_solve(solver.h, _lib.field_ptrs(q, solver.ns), float(timeend),

@@ -27,8 +27,13 @@ tendency launch per LSRK stage:
   steps any of its requests still needs (capped by ``max_tick_steps``), so
   every request takes exactly its own step count; the launches of one tick are
   captured once per (launched prefix, S) into a CUDA graph and replayed;
-* a finished request's state is copied to pinned host memory and its latency
-  (arrival to result on the host) recorded.
+* a request's inputs may stay on the device: ``make`` builds its initial state
+  and aux fields there at admission (on the copy stream), or ``q0`` / ``aux``
+  are CUDA tensors; only the small geometry tables cross PCIe;
+* a finished request returns what its client asks for: the whole state copied
+  to pinned host memory (``result_mode="state"``), or its per-component
+  MJ-weighted L2 norms computed on the device (``"norms"``, Ns doubles); its
+  latency (arrival to result on the host) is recorded.
 
 Each request's result is bitwise the one it gets stepped alone: every node of
 it sees the same operands in the same order whatever shares its pool.
@@ -41,7 +46,7 @@ import ctypes as C
 import math
 import time
 from dataclasses import dataclass, field
-from typing import Dict, List, Optional, Tuple
+from typing import Callable, Dict, List, Optional, Tuple
 
 import numpy as np
 
@@ -69,11 +74,16 @@ _GRID_FIELDS = ("K", "vertices", "periodic", "stacked")
 class Request:
     rid: int
     dg: object                 # DGSEM spec of this instance
-    q0: np.ndarray             # (Ns, K, Np) float64 initial state
+    q0: object                 # (Ns, K, Np) float64 initial state: numpy (host) or a CUDA tensor; None with make
     dt: float
     nsteps: int
     arrival: float = 0.0       # seconds after the stream starts
-    keep_result: bool = True   # False: the final state is copied out, then dropped
+    keep_result: bool = True   # False: the result is copied out, then dropped
+    # () -> (q0, aux): CUDA tensors (Ns, K, Np) and (naux, K, Np) or None, built
+    # on the device at admission, on the server's copy stream
+    make: Optional[Callable] = None
+    aux: object = None         # aux fields (host array or CUDA tensor); default: dg.auxstate_host()
+    result_mode: str = "state"  # "state": the final state; "norms": its per-component weighted L2 norms
     # filled by the server
     admitted: float = math.nan
     finished: float = math.nan
@@ -85,7 +95,7 @@ class Request:
 
     @property
     def dof(self) -> int:
-        return int(np.prod(self.q0.shape))
+        return int(self.dg.law.numberofstates * self.dg.grid.K * self.dg.grid.cell.Np)
 
 
 def kind_key(dg) -> tuple:
@@ -111,6 +121,27 @@ def pool_bytes_per_element(dg) -> int:
     return 8 * Np * (3 * ns + max(1, naux)) + (3 * 8 + 8 + 6 * 4 + 8)
 
 
+def _element_weights(dg, device):
+    """Per-element Jacobians J (K) and per-node LGL weights w (Np) of a brick
+    grid on the device: MJ = J (x) w (src/dgsem.jl:43-45), cached on the spec."""
+    import torch
+
+    jw = getattr(dg, "_serve_jw", None)
+    if jw is None or jw[0].device != device:
+        g, c = dg.grid, dg.grid.cell
+        eidx = g.element_indices()
+        J = np.ones(len(g))
+        for d in range(g.dim):
+            J = J * (np.diff(g.vertices[d])[eidx[:, d]] / 2)
+        node = np.arange(c.Np)
+        w = np.ones(c.Np)
+        for d in range(g.dim):
+            w = w * c.weights[(node // c.Nq ** d) % c.Nq]
+        jw = (torch.as_tensor(J, device=device), torch.as_tensor(w, device=device))
+        dg._serve_jw = jw
+    return jw
+
+
 class _Placed:
     __slots__ = ("req", "first", "K", "remaining", "desc", "keep", "aux")
 
@@ -120,7 +151,12 @@ class _Placed:
         self.K = req.dg.grid.K
         self.remaining = int(req.nsteps)
         self.desc, self.keep = make_desc(req.dg)
-        self.aux = np.ascontiguousarray(req.dg.auxstate_host(), dtype=np.float64).reshape(-1)
+        if req.make is not None:
+            self.aux = None  # built on the device at admission
+        elif req.aux is not None:
+            self.aux = req.aux
+        else:
+            self.aux = np.ascontiguousarray(req.dg.auxstate_host(), dtype=np.float64).reshape(-1)
 
 
 class _PoolDevice:
@@ -270,9 +306,19 @@ class _Pool:
         return self.capacity - self._free_start()
 
     # admission ----------------------------------------------------------
-    def _place(self, p: _Placed, stream):
-        _lib.check(_lib.lib().atb_op_place_instance(self._dev.h, p.first, C.byref(p.desc),
-                                                    _lib.dptr(p.aux) if p.aux.size else None,
+    def _place(self, p: _Placed, stream, aux=None):
+        """Geometry and aux fields of a placement; ``aux``: host array or CUDA
+        tensor (default: the placement's host aux)."""
+        import torch
+
+        a = p.aux if aux is None else aux
+        if isinstance(a, torch.Tensor):
+            if a.dtype != torch.float64 or not a.is_contiguous():
+                raise TypeError("device aux fields must be contiguous float64")
+            ptr = C.cast(C.c_void_p(a.data_ptr()), _lib._DP) if a.numel() else None
+        else:
+            ptr = _lib.dptr(a) if a is not None and a.size else None
+        _lib.check(_lib.lib().atb_op_place_instance(self._dev.h, p.first, C.byref(p.desc), ptr,
                                                     _lib.stream_ptr(stream)))
 
     def admit(self, r: Request, now: float):
@@ -283,6 +329,28 @@ class _Pool:
         p = _Placed(r, self._free_start())
         K = p.K
         n = self.ns * K * self.Np
+        dev_q0 = isinstance(r.q0, torch.Tensor) and r.q0.is_cuda
+        if r.make is not None or dev_q0:
+            # inputs on the device: built there now (make) or handed over as
+            # CUDA tensors; device-to-device copies on the copy stream
+            if r.make is None:
+                # the caller's tensors were written on its current stream
+                self.copy_stream.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(self.copy_stream):
+                if r.make is not None:
+                    q0, aux = r.make()
+                else:
+                    q0 = r.q0
+                    aux = r.aux if isinstance(r.aux, torch.Tensor) else None
+                self._place(p, self.copy_stream, aux=aux.reshape(-1) if aux is not None else None)
+                self.q[:, p.first:p.first + K].copy_(q0.reshape(self.ns, K, self.Np), non_blocking=True)
+                ev = self.copy_stream.record_event()
+            self.pending.append(ev)
+            self.placed.append(p)
+            self.used = p.first + K
+            r.admitted = now
+            self.dirty = True
+            return
         src = None
         if isinstance(r.q0, np.ndarray) and r.q0.dtype == np.float64 and r.q0.flags.c_contiguous:
             t = torch.from_numpy(r.q0.reshape(-1))
@@ -381,14 +449,23 @@ class _Pool:
         outs = []
         buf = None
         if fin:
-            tot = sum(self.ns * p.K * self.Np for p in fin)
+            size = lambda p: self.ns * p.K * self.Np if p.req.result_mode == "state" else self.ns  # noqa: E731
+            tot = sum(size(p) for p in fin)
             buf, token = self.results.get(tot)
             o = 0
             with torch.cuda.stream(self.stream):
                 for p in fin:
-                    m = self.ns * p.K * self.Np
-                    v = buf[o:o + m].view(self.ns, p.K, self.Np)
-                    v.copy_(self.q[:, p.first:p.first + p.K], non_blocking=True)
+                    m = size(p)
+                    if p.req.result_mode == "state":
+                        v = buf[o:o + m].view(self.ns, p.K, self.Np)
+                        v.copy_(self.q[:, p.first:p.first + p.K], non_blocking=True)
+                    else:
+                        # per-component sqrt(sum MJ q^2) on the device; Ns doubles to the host
+                        J, w = _element_weights(p.req.dg, self.cuda)
+                        x = self.q[:, p.first:p.first + p.K]
+                        nrm = torch.stack([torch.dot(J, torch.mv(x[c] * x[c], w)) for c in range(self.ns)]).sqrt()
+                        v = buf[o:o + m]
+                        v.copy_(nrm, non_blocking=True)
                     outs.append((p.req, v))
                     o += m
             t3 = time.perf_counter()
@@ -569,6 +646,15 @@ class Server:
         if not realtime:
             for r in reqs:
                 r.arrival = 0.0
+        # statistics cover this run only (pools persist across runs)
+        self.retired_updates = 0
+        self.timers = {k: 0.0 for k in self.timers}
+        self.peak_bytes = self.pool_bytes
+        self.pools_made = 0
+        for ps in self.pools.values():
+            for p in ps:
+                p.dof_stage_updates = 0
+                p.host = {k: 0.0 for k in p.host}
         queue: List[Request] = []
         done: List[Request] = []
         torch.cuda.synchronize()

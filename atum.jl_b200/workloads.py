@@ -204,3 +204,51 @@ def sw_fplane(N=4, K=32, L=1.0e6, H=100.0, seed=20261203, lake_at_rest=False, pr
     dx = L / K
     dt = 0.3 * dx / N / (np.sqrt(g * np.max(h)))
     return Case("sw_fplane", dg, q0, dt, steps * dt, extra={"steps": steps})
+
+
+# --------------------------------------------- device-built initial states
+def vortex_c1_device(dg):
+    """The vortex of ``vortex_c1`` on ``dg``'s grid, built on the device:
+    (q0, aux) CUDA tensors (the Euler law has no aux fields)."""
+    import torch
+    from .cell import points_device
+
+    x = points_device(dg.grid)
+    g = dg.law.gamma
+    r0 = x[0] - 10.0 * torch.round(x[0] / 10.0)
+    r1 = x[1] - 10.0 * torch.round(x[1] / 10.0)
+    f = 5.0 * torch.exp(1 - (r0 * r0 + r1 * r1))
+    rho = (1 - (g - 1) * f ** 2 / (16 * g * math.pi ** 2)) ** (1 / (g - 1))
+    m0 = rho * (1.0 + f / (2 * math.pi) * (-r1))
+    m1 = rho * (1.0 + f / (2 * math.pi) * r0)
+    E = rho ** g / (g - 1) + (m0 * m0 + m1 * m1) / (2 * rho)
+    return torch.stack([rho, m0, m1, E]).contiguous(), None
+
+
+def bubble_3d_device(dg, L=10e3):
+    """The rising bubble of ``bubble_3d`` on ``dg``'s grid, built on the
+    device: (q0, aux) CUDA tensors, aux = [Phi, grad Phi, rho_ref, p_ref] of
+    the constant-theta background (src/balancelaws/euler_gravity.jl:38-62)."""
+    import torch
+    from .cell import points_device
+
+    law = dg.law
+    grav = law.grav
+    cv = 719.0
+    cp = law.gamma * cv
+    R = cp - cv
+    x = points_device(dg.grid)
+    z = x[2]
+    pi_ex = 1 - grav / (cp * 300.0) * z
+    aux = torch.zeros((law.naux,) + tuple(z.shape), dtype=torch.float64, device=z.device)
+    aux[0] = grav * z
+    aux[3] = grav
+    aux[4] = 1e5 / (R * 300.0) * pi_ex ** (cv / R)
+    aux[5] = 1e5 * pi_ex ** (cp / R)
+    r = torch.sqrt((x[0] - L / 2) ** 2 + (x[1] - L / 2) ** 2 + (z - 2000.0) ** 2)
+    theta = 300.0 + 2.0 * torch.exp(-(r / 2000.0) ** 2)
+    p = 1e5 * pi_ex ** (cp / R)
+    rho = p / (R * (theta * pi_ex))
+    zero = torch.zeros_like(rho)
+    rhoe = p / (law.gamma - 1) + rho * aux[0]
+    return torch.stack([rho, zero, zero, zero, rhoe]).contiguous(), aux.contiguous()

@@ -37,6 +37,7 @@ extern "C" {
 #define ATB_ERR_NONFINITE (-4)   /* NaN/Inf detected in a state */
 #define ATB_ERR_BUDGET (-5)      /* serving: request exceeds the HBM budget */
 #define ATB_ERR_TIMEOUT (-6)     /* bounded device wait expired */
+#define ATB_ERR_CALLBACK (-7)    /* a stage callback returned nonzero */
 
 /* law: src/balancelaws/{advection,euler,euler_gravity,linear_euler_gravity,shallow_water}.jl */
 #define ATB_LAW_ADVECTION 0
@@ -148,9 +149,9 @@ int atb_op_set_active(atb_op* op, int n_instances);
  * the geometry (metrics, neighbour table offset by first_element) and aux
  * fields of the instance `desc` (same kind, any grid) into elements
  * [first_element, first_element + K) with copies ordered on `stream` (the
- * geometry goes through the pool's own page-locked staging; a pageable aux
- * source may be released on return, a page-locked one must stay valid until
- * the copies have run).  atb_op_set_active_elements sets how
+ * geometry goes through the pool's own page-locked staging; aux_host may be
+ * host or device memory: a pageable host source may be released on return, a
+ * page-locked or device one must stay valid until the copies have run).  atb_op_set_active_elements sets how
  * many leading elements tendency launches cover; a caller keeps its placed
  * instances inside that prefix.  Pools have no banded solve (ARK23). */
 int atb_op_create_pool(const atb_op_desc* kind, int capacity_elements, atb_op** out);
@@ -217,6 +218,25 @@ int atb_solver_set_instance_dt(atb_solver* s, const double* dt_host);
  * solver that cannot fuse is an error. */
 int atb_solver_fuse(atb_solver* s, int enable);
 int atb_solver_set_element_dt(atb_solver* s, const double* dte_device);
+
+/* after_stage of solve!(q, timeend, solver; after_stage) -- src/odesolvers.jl:
+ * 10-11,23, called at :54 (LSRK), :119 (RLSRK) and :378 (ARK).  With a
+ * callback set, every atb_solver_step / atb_solve calls
+ *   cb(ex_time, im_time, q_stage, user)
+ * on the host after each stage's launches have been enqueued on the call's
+ * stream: LSRK / RLSRK after every stage, with both times the stage time and
+ * q_stage the caller's q (the callback may change it; the next stage starts
+ * from it); ARK23 after stages 2 and 3, with the explicit and implicit stage
+ * times and q_stage the solver's stage state Q_i (Ns device pointers, valid
+ * during the call).  A callback that reads device memory from the host must
+ * synchronise the stream first; device work it enqueues on that stream is
+ * ordered before the next stage.  A nonzero return stops the step with
+ * ATB_ERR_CALLBACK.  With the accumulated ARK23 path (split_rhs = 0 with a
+ * banded solve) the step's update of q is already applied when the stage-3
+ * callback runs.  NULL clears the callback.  (No counterpart in the C sense:
+ * the reference passes a Julia closure.) */
+typedef int (*atb_stage_callback)(double ex_time, double im_time, double* const* q_stage, void* user);
+int atb_solver_set_stage_callback(atb_solver* s, atb_stage_callback cb, void* user);
 
 /* measures -- src/measures.jl:6-33 (p = 2 or INFINITY); results to host memory */
 int atb_weightednorm(atb_op* op, const double* const* q, double p, double* comp_host, double* total_host,

@@ -597,6 +597,9 @@ struct Solver {
   int bw = 0, nunk = 0, nlines = 0;
   std::vector<double> band;
   std::vector<size_t> line_map;  // nlines x nunk -> global index (state-major offset)
+  // after_stage (src/odesolvers.jl:10-11,23): called after every stage
+  orc_stage_cb stage_cb = nullptr;
+  void* stage_user = nullptr;
 };
 
 void coeffs_lsrk54(Solver& s) {
@@ -631,6 +634,7 @@ void lsrk_step(Solver& s, double* q) {
     op_apply(*s.rhs, s.dq.data(), q, stagetime, true);
     double c = s.rkb[st] * s.dt;
     for (size_t i = 0; i < n; ++i) q[i] = q[i] + c * s.dq[i];
+    if (s.stage_cb) s.stage_cb(stagetime, stagetime, q, s.stage_user);  // src/odesolvers.jl:54
   }
   s.time += s.dt;
 }
@@ -649,6 +653,7 @@ void rlsrk_step(Solver& s, double* q) {
     deta = deta + s.rkb_full[st] * s.dt * entropyproduct(o, q, s.k.data());
     double c = s.rkb[st] * s.dt;
     for (size_t i = 0; i < n; ++i) q[i] = q[i] + c * s.dq[i];
+    if (s.stage_cb) s.stage_cb(stagetime, stagetime, q, s.stage_user);  // src/odesolvers.jl:119
   }
   for (size_t i = 0; i < n; ++i) s.k[i] = q[i] - s.q0[i];
   // nlsolve(r, dr, [gamma]; ftol = 10 eps) with NLsolve's default
@@ -821,6 +826,8 @@ void ark_step(Solver& s, double* q) {
     else
       std::memcpy(Q[i], s.Qhat.data(), n * sizeof(double));
     eval(i, Q[i]);
+    // src/odesolvers.jl:378: after stages 2..s, with both stage times
+    if (s.stage_cb) s.stage_cb(s.time + s.exc[i] * s.dt, s.time + s.imc[i] * s.dt, Q[i], s.stage_user);
   }
   for (int i = 0; i < 3; ++i)
     for (size_t j = 0; j < n; ++j) q[j] = q[j] + s.dt * (s.exb[i] * s.exK[i][j] + s.imb[i] * s.imK[i][j]);
@@ -944,6 +951,10 @@ int orc_solve(void* sv, double* q, double timeend, int adjust_final) {
 }
 void orc_step(void* sv, double* q, int nsteps) {
   for (int i = 0; i < nsteps; ++i) solver_step(*(Solver*)sv, q);
+}
+void orc_set_stage_callback(void* sv, orc_stage_cb cb, void* user) {
+  ((Solver*)sv)->stage_cb = cb;
+  ((Solver*)sv)->stage_user = user;
 }
 double orc_solver_time(void* s) { return ((Solver*)s)->time; }
 double orc_solver_dt(void* s) { return ((Solver*)s)->dt; }

@@ -53,6 +53,12 @@ void* orc_solver_create(int kind, void* rhs, void* linrhs, double dt, double t0,
 void orc_solver_destroy(void* s);
 int orc_solve(void* s, double* q, double timeend, int adjust_final); /* returns steps taken */
 void orc_step(void* s, double* q, int nsteps);
+/* after_stage (src/odesolvers.jl:10-11,23,54,119,378): cb(ex_time, im_time,
+ * stage state, user) after every LSRK / RLSRK stage (both times the stage
+ * time, the state q) and after ARK23 stages 2 and 3 (the stage state Q_i);
+ * NULL clears it */
+typedef void (*orc_stage_cb)(double ex_time, double im_time, const double* q_stage, void* user);
+void orc_set_stage_callback(void* s, orc_stage_cb cb, void* user);
 double orc_solver_time(void* s);
 double orc_solver_dt(void* s);
 double orc_solver_gamma(void* s);

@@ -18,6 +18,8 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
+# void (*)(double ex_time, double im_time, const double* q_stage, void* user)
+_STAGE_CB = C.CFUNCTYPE(None, C.c_double, C.c_double, C.POINTER(C.c_double), C.c_void_p)
 
 
 class _Desc(C.Structure):
@@ -70,6 +72,7 @@ def lib():
         L.orc_entropyproduct.argtypes = [vp, dp, dp]
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_count_flops.argtypes = [C.POINTER(_Desc), C.c_int, C.c_int, dp, dp, dp, dp, dp, C.POINTER(C.c_long)]
+        L.orc_set_stage_callback.argtypes = [vp, _STAGE_CB, vp]
         _LIB = L
     return _LIB
 
@@ -174,6 +177,23 @@ class Solver:
 
     def step(self, q: np.ndarray, nsteps: int = 1):
         lib().orc_step(self.h, _dp(q), int(nsteps))
+
+    def set_after_stage(self, fn):
+        """``fn(ex_time, im_time, q_stage)`` after every stage (LSRK / RLSRK)
+        or after ARK23 stages 2 and 3, as the reference's ``after_stage``;
+        ``q_stage`` is a copy of the stage state.  None clears it."""
+        if fn is None:
+            self._cb = None
+            lib().orc_set_stage_callback(self.h, _STAGE_CB(), None)
+            return
+        n = self.rhs.ns * self.rhs.K * self.rhs.Np if self.rhs is not None else \
+            self.linrhs.ns * self.linrhs.K * self.linrhs.Np
+
+        def cb(ex_t, im_t, qp, user):
+            fn(ex_t, im_t, np.ctypeslib.as_array(qp, shape=(n,)).copy())
+
+        self._cb = _STAGE_CB(cb)
+        lib().orc_set_stage_callback(self.h, self._cb, None)
 
 
 def LSRK54(dg, q, dt, t0=0.0):

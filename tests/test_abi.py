@@ -79,20 +79,3 @@ def test_solver_rejects_unusable_dt_without_gpu(dt):
     assert rc == -1
     assert b"dt must be finite and positive" in L.atb_last_error()
     assert not h.value
-
-
-@pytest.mark.parametrize("sflux", ["roe", "matrix", "ec"])
-def test_fp32flux_with_unported_surface_flux_rejected_without_gpu(sflux):
-    """The FP32-flux form has FP32 arithmetic for the central and Rusanov
-    surface fluxes only; other surface fluxes are refused (not silently run in
-    FP64)."""
-    from atum_b200 import _lib, _device
-    flux = {"roe": A.RoeFlux(), "matrix": A.MatrixFlux(), "ec": A.EntropyConservativeFlux()}[sflux]
-    dg = A.DGSEM(law=A.EulerLaw(2), grid=A.brickgrid(A.LobattoCell(3, 3), ([0, 1, 2], [0, 1, 2])),
-                 surface_numericalflux=flux, volume_form=A.FluxDifferencingForm(A.EntropyConservativeFlux()),
-                 precision="fp32flux")
-    d, keep = _device.make_desc(dg)
-    h = C.c_void_p()
-    rc = _lib.lib().atb_op_create(C.byref(d), None, C.byref(h))
-    assert rc == -1
-    assert b"central and Rusanov surface fluxes only" in _lib.lib().atb_last_error()

@@ -103,3 +103,60 @@ def test_fp32flux_rejected_where_not_built():
     dg = A.DGSEM(law=A.EulerLaw(2), grid=grid, surface_numericalflux=A.RusanovFlux(), precision="fp32flux")
     with pytest.raises(A._lib.AtbError):
         dg.device
+
+
+_SFLUX = {"ec": A.EntropyConservativeFlux(), "kg": A.KennedyGruberFlux(), "roe": A.RoeFlux(),
+          "matrix": A.MatrixFlux()}
+
+
+@pytest.mark.parametrize("law,sflux", [("euler", "roe"), ("euler", "matrix"), ("euler", "ec"), ("euler", "kg"),
+                                       ("eg", "roe"), ("eg", "matrix"), ("eg", "ec"), ("sw", "roe"),
+                                       ("sw", "ec"), ("sw_topo", "roe"), ("sw_topo", "ec")])
+def test_fp32flux_surface_fluxes(law, sflux):
+    """Every surface flux has an FP32-flux form (src/balancelaws/euler.jl:91-138,
+    198-256; euler_gravity.jl:149-198,271-332; shallow_water.jl:68-136): one
+    operator application within 1e-6 of FP64 (field-relative per component),
+    and not bitwise equal to it (the FP32 arithmetic runs)."""
+    from test_gpu_parity import make_dg
+    dim = 2
+    kw = dict(bc="reflect") if law == "eg" else {}
+    d64 = make_dg(law, dim, 3, 3, "ec", sflux, **kw)
+    d32 = A.DGSEM(law=d64.law, grid=d64.grid, volume_form=d64.volume_form, surface_numericalflux=_SFLUX[sflux],
+                  precision="fp32flux")
+    q = PT.random_state(d64)
+    a, b = PT.to_dev(np.zeros_like(q)), PT.to_dev(np.zeros_like(q))
+    d64(a, PT.to_dev(q), 0.0, increment=False)
+    d32(b, PT.to_dev(q), 0.0, increment=False)
+    ha, hb = PT.to_host(a), PT.to_host(b)
+    err = PT.field_rel_errors(hb, ha)
+    assert np.all(err <= 1e-6), err
+    assert not np.array_equal(ha, hb)
+
+
+@pytest.mark.parametrize("sflux", ["roe", "matrix"])
+def test_vortex_fp32flux_roe_matrix(sflux):
+    """The isentropic vortex (C1) stepped 100 LSRK54 steps with a Roe or
+    Matrix surface flux: FP32-flux form within 1e-6 (relative L2) of FP64."""
+    c64 = P.vortex_c1()
+    d64 = A.DGSEM(law=c64.dg.law, grid=c64.dg.grid, volume_form=c64.dg.volume_form,
+                  surface_numericalflux=_SFLUX[sflux])
+    d32 = A.DGSEM(law=c64.dg.law, grid=c64.dg.grid, volume_form=c64.dg.volume_form,
+                  surface_numericalflux=_SFLUX[sflux], precision="fp32flux")
+    q64, q32 = PT.to_dev(c64.q0), PT.to_dev(c64.q0)
+    A.LSRK54(d64, q64, c64.dt).step(q64, 100)
+    A.LSRK54(d32, q32, c64.dt).step(q32, 100)
+    assert _rel(d64, q32, q64) <= 1e-6
+
+
+def test_lake_at_rest_fp32flux_roe_ec():
+    """The well-balanced bathymetry terms stay FP64 in the FP32-flux Roe and
+    EC surface fluxes: a lake at rest stays at rest to round-off."""
+    import torch
+    for sflux in ("roe", "ec"):
+        c = P.sw_fplane(K=8, steps=50, precision="fp32flux", lake_at_rest=True)
+        dg = A.DGSEM(law=c.dg.law, grid=c.dg.grid, volume_form=c.dg.volume_form,
+                     surface_numericalflux=_SFLUX[sflux], precision="fp32flux")
+        q = PT.to_dev(c.q0)
+        A.LSRK54(dg, q, c.dt).step(q, 50)
+        umax = float(q[1:3].abs().max() / q[0].abs().max())
+        assert umax <= 1e-12, (sflux, umax)

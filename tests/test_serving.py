@@ -132,3 +132,53 @@ def test_pool_place_rejects_other_kind_and_overflow():
         assert _lib.lib().atb_op_set_active_elements(h, 21) != 0
     finally:
         _lib.lib().atb_op_destroy(h)
+
+
+@pytest.mark.parametrize("graphs", [False, True])
+def test_device_built_inputs_and_norm_results(graphs):
+    """Requests whose initial state and aux fields are built on the device at
+    admission (``make``), mixed with host-input requests: each served state is
+    bitwise the state stepped alone from the same inputs, and a request that
+    asks for norms gets the per-component MJ-weighted L2 norms of that state."""
+    import torch
+    from atum_b200 import workloads as W
+    reqs = []
+    for i in range(10):
+        if i % 2:
+            c = P.bubble_3d(N=2, K=3, imex=False, precision="fp32flux" if i % 3 else "fp64")
+            make = (lambda dg=c.dg: W.bubble_3d_device(dg))
+        else:
+            c = P.vortex_c1(N=3, K=4)
+            make = (lambda dg=c.dg: W.vortex_c1_device(dg))
+        mode = "norms" if i % 4 == 3 else "state"
+        reqs.append(A.serving.Request(rid=i, dg=c.dg, q0=None, make=make, dt=c.dt, nsteps=3 + i, arrival=0.0,
+                                      result_mode=mode))
+    srv = A.serving.Server(capacity=96, chunk=16, use_graphs=graphs, max_tick_steps=4)
+    st = srv.run(reqs, realtime=False)
+    assert st.requests == 10
+    for r in reqs:
+        q0, aux = r.make()
+        if aux is not None:
+            # the device-built aux equals the host-evaluated one
+            assert np.allclose(PT.to_host(aux), r.dg.auxstate_host(), rtol=1e-14, atol=1e-12)
+        q = q0.clone()
+        A.LSRK54(r.dg, q, r.dt).step(q, r.nsteps)
+        torch.cuda.synchronize()
+        alone = PT.to_host(q)
+        if r.result_mode == "state":
+            assert np.array_equal(r.result, alone), r.rid
+        else:
+            mj = r.dg.MJ
+            ref = np.sqrt([np.sum(mj * alone[c] ** 2) for c in range(alone.shape[0])])
+            assert r.result.shape == ref.shape
+            assert np.allclose(r.result, ref, rtol=1e-13, atol=0), r.rid
+    srv.close()
+
+
+def test_device_built_states_match_host_builders():
+    """The device builders of the serving workload restate the host ones."""
+    from atum_b200 import workloads as W
+    for c, fn in ((P.vortex_c1(N=3, K=4), W.vortex_c1_device), (P.bubble_3d(N=3, K=3, imex=False),
+                                                                W.bubble_3d_device)):
+        q0, _ = fn(c.dg)
+        assert np.allclose(PT.to_host(q0), c.q0, rtol=1e-14, atol=1e-12)
