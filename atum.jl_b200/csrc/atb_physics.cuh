@@ -643,18 +643,31 @@ __device__ __forceinline__ void matrix_diss32(const LawP& L, int d, double sgn, 
   double vm[NS], vp[NS];
   entropyvars<LAW, DIM>(L, qm, am, vm);
   entropyvars<LAW, DIM>(L, qp, ap, vp);
+  double dv64[NS];
   float dv[NS];
 #pragma unroll
-  for (int s = 0; s < NS; ++s) dv[s] = (float)(vp[s] - vm[s]);
+  for (int s = 0; s < NS; ++s) {
+    dv64[s] = vp[s] - vm[s];
+    dv[s] = (float)dv64[s];
+  }
   const float l1 = fabsf(un - c_bar) * rho_log / (2.f * g);
   const float l2 = fabsf(un) * rho_log * (g - 1.f) / g;
   const float l3 = fabsf(un + c_bar) * rho_log / (2.f * g);
   const float l4 = fabsf(un) * p_avg;
   float k2 = u2_bar / 2.f;
   if (LAW == LAW_EG) k2 += Phi_avg;
-  const float w1 = l1 * (dv[0] + dot<DIM>(umc, dv + 1) + (h_bar - c_bar * un) * dv[DIM + 1]);
-  const float w2 = l2 * (dv[0] + dot<DIM>(ua, dv + 1) + k2 * dv[DIM + 1]);
-  const float w3 = l3 * (dv[0] + dot<DIM>(upc, dv + 1) + (h_bar + c_bar * un) * dv[DIM + 1]);
+  // the three projections of the entropy-variable jump cancel to a few
+  // times their terms' size (the enthalpy-like h_bar times the jump of -2b
+  // against the jump of the first entropy variable): summed in FP64
+  auto proj = [&](const float* a, float hh) {
+    double t = dv64[0] + (double)hh * dv64[DIM + 1];
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) t += (double)a[k] * dv64[1 + k];
+    return (float)t;
+  };
+  const float w1 = l1 * proj(umc, h_bar - c_bar * un);
+  const float w2 = l2 * proj(ua, k2);
+  const float w3 = l3 * proj(upc, h_bar + c_bar * un);
   const float ndv = dot<DIM>(n, dv + 1);
   Dm[0] = w1 + w2 + w3;
 #pragma unroll

@@ -284,13 +284,15 @@ __device__ __forceinline__ void face_task(const TendArgs& A, const LawP& L, int 
 // arithmetic folds, line loops unroll); NQ_ = 0 reads it from the arguments.
 // CTA size limit of the fused kernels: 256 threads unless one element needs
 // more; with the compact layout at Nq = 5 (125 nodes), one element per CTA of
-// 128 threads and five CTAs per SM (43 KB of shared memory each, 96 registers).
-// cmp: the kernel uses the compact layout (fused_compact_fits).
+// 128 threads, four CTAs per SM at the full 128-register budget (measured on
+// B200: faster than five CTAs at 96 registers, whose spills cost more than
+// the added warps gain).  cmp: the kernel uses the compact layout
+// (fused_compact_fits).
 __host__ __device__ constexpr int fused_max_threads(int nq, bool cmp = false) {
   return (nq == 0 || nq * nq * nq > 256) ? 512 : (cmp && nq == 5) ? 128 : 256;
 }
 __host__ __device__ constexpr int fused_min_blocks(int nq, bool cmp = false) {
-  return (cmp && nq == 5) ? 5 : 512 / fused_max_threads(nq, cmp);
+  return (cmp && nq == 5) ? 4 : 512 / fused_max_threads(nq, cmp);
 }
 
 // Plain launches: up to 512 threads.  Fused launches (which carry the linear
@@ -522,10 +524,11 @@ __global__ void __launch_bounds__(
     if constexpr (PAIRS) {
       // ---- phase A: each unordered pair of each line of direction d once
       if (act) {
-        // two pairs per thread per direction at N=4: unrolled, the fused ARK
-        // kernel interleaves their flux chains (measured 3% faster); the
-        // plain kernel is faster rolled
-#pragma unroll(FUSE ? 2 : 1)
+        // rolled: the instruction stream stays small (unrolling by two
+        // interleaves the flux chains of a thread's pairs, but the larger
+        // kernel body stalls on instruction fetch; measured 5% slower for
+        // the fused ARK stage kernel on B200)
+#pragma unroll 1
         for (int t = node; t < Nfp * npl; t += Np) {
           const int line = t / npl, p = t - line * npl;
           const int lb = (d == 0) ? line * Nq : (d == 1) ? (line % Nq) + Nq * Nq * (line / Nq) : line;
