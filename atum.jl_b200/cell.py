@@ -179,6 +179,17 @@ def points_device(grid: "BrickGrid", device="cuda"):
 
     c = grid.cell
     dim, Nq, Np, K, Kd = grid.dim, c.Nq, c.Np, grid.K, grid.Kd
+    # the node and vertex tables are copied to the device once per grid (a
+    # copy from pageable host memory makes the host wait for the stream)
+    dev = torch.device(device)
+    if dev.type == "cuda" and dev.index is None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+    cache = grid.__dict__.setdefault("_device_tables", {})
+    if dev not in cache:
+        cache[dev] = (torch.as_tensor(np.asarray(c.nodes, dtype=np.float64), device=dev),
+                      [torch.as_tensor(np.asarray(grid.vertices[d], dtype=np.float64), device=dev)
+                       for d in range(dim)])
+    nodes, verts = cache[dev]
     e = torch.arange(K, device=device, dtype=torch.int64)
     idx = [None] * dim
     if grid.stacked:
@@ -193,10 +204,9 @@ def points_device(grid: "BrickGrid", device="cuda"):
             idx[d] = r % Kd[d]
             r = r // Kd[d]
     node = torch.arange(Np, device=device, dtype=torch.int64)
-    nodes = torch.as_tensor(np.asarray(c.nodes, dtype=np.float64), device=device)
     x = torch.empty((dim, K, Np), dtype=torch.float64, device=device)
     for d in range(dim):
-        v = torch.as_tensor(np.asarray(grid.vertices[d], dtype=np.float64), device=device)
+        v = verts[d]
         v0 = v[idx[d]][:, None]
         v1 = v[idx[d] + 1][:, None]
         xi = nodes[(node // Nq ** d) % Nq][None, :]

@@ -910,15 +910,6 @@ struct atb_solver {
   double* blk = nullptr;
   double* frag = nullptr;
   int ld = 0;
-  // twisted solve from both ends of each column (atb_band.cu): the reversed
-  // column's factor, its blocks and tiles, the middle element's tiles, and a
-  // per-line buffer for the middle right-hand side and coupling rows
-  double* bandf = nullptr;
-  double* blkf = nullptr;
-  double* fragf = nullptr;
-  double* fragm = nullptr;
-  double* rmid = nullptr;
-  int mid = 0;
   // ARK23 stages fused into one kernel per stage (explicit tendency + linear
   // operator), when the two operators allow it (atb_solver_fuse)
   tend_launch_fn fused = nullptr;
@@ -945,11 +936,6 @@ void solver_free(atb_solver* s) {
   cudaFree(s->band);
   cudaFree(s->blk);
   cudaFree(s->frag);
-  cudaFree(s->bandf);
-  cudaFree(s->blkf);
-  cudaFree(s->fragf);
-  cudaFree(s->fragm);
-  cudaFree(s->rmid);
   if (s->own_dte) cudaFree(s->d_dte);
   delete s;
 }
@@ -985,123 +971,6 @@ int copy_field(double* const* dst, const double* const* src, int ns, size_t n, c
   for (int s = 0; s < ns; ++s)
     CK(cudaMemcpyAsync(dst[s], src[s], n * sizeof(double), cudaMemcpyDeviceToDevice, st));
   return ATB_OK;
-}
-
-// The twisted solve's data (atb_band.cu, band_solve_twist_kernel): the
-// factor of the column read backwards (the same no-pivot banded LU of the
-// reversed unfactored band), its block inverses and tiles, and the middle
-// element m = KV/2: P = S_m + S'_m - D_m from the two factors' Schur
-// complements S_m = L_mm U_mm (forward) and S'_m (backward, reversed back)
-// and the block D_m of I - dt a L; its inverse and -P^-1 C_top,
-// -P^-1 C_bottom (C: the factors' couplings of element m to its neighbours)
-// as matrix-unit tiles.  Computed once per solver; leaves s->fragf null (the
-// whole-column sweep runs) when the reversed blocks or the couplings lack the
-// face-node zero structure.  a_host: the unfactored compact band.
-int build_twist(atb_solver* s, const std::vector<double>& a_host, double scale, cudaStream_t st) {
-  const LineMap& M = s->M;
-  const int BW1 = M.bw + 1, bw = M.bw, n = M.nunk, NS = M.ns, KV = M.KV;
-  const size_t rs = 2 * (size_t)(M.bw + 1);
-  int rc;
-  double* rev = nullptr;
-  if ((rc = dalloc(&rev, (size_t)n * rs))) return rc;
-  CK(cudaMemcpyAsync(rev, a_host.data(), a_host.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-  if ((rc = dalloc(&s->bandf, (size_t)n * rs))) { cudaFree(rev); return rc; }
-  launch_band_reverse(rev, n, bw, s->bandf, st);
-  launch_band_factor(n, bw, 1, s->bandf, (int)rs, 1, scale, st);
-  if ((rc = dalloc(&s->blkf, (size_t)KV * 4 * BW1 * BW1))) { cudaFree(rev); return rc; }
-  launch_block_prep(s->bandf, KV, BW1, s->blkf, st);
-  std::vector<double> hblk((size_t)KV * 4 * BW1 * BW1), F((size_t)n * rs), Fr((size_t)n * rs);
-  CK(cudaMemcpyAsync(hblk.data(), s->blkf, hblk.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
-  CK(cudaMemcpyAsync(F.data(), s->band, F.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
-  CK(cudaMemcpyAsync(Fr.data(), s->bandf, Fr.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  cudaFree(rev);
-  auto drop = [&]() {
-    cudaFree(s->bandf);
-    cudaFree(s->blkf);
-    s->bandf = s->blkf = nullptr;
-    return ATB_OK;
-  };
-  if (!warp_solve_structure_ok(hblk.data(), KV, BW1, NS)) return drop();
-  // entry (i, j) of a compact band (zero outside the band)
-  auto at = [&](const std::vector<double>& b, int i, int j) -> double {
-    const int o = j - i + bw;
-    return (o < 0 || o > 2 * bw) ? 0.0 : b[(size_t)i * rs + o];
-  };
-  const int m = KV / 2, mr = KV - 1 - m;  // middle element; its index in the reversed column
-  const int r0 = m * BW1, q0 = mr * BW1;
-  std::vector<double> P((size_t)BW1 * BW1), CT((size_t)BW1 * BW1), CB((size_t)BW1 * BW1);
-  for (int i = 0; i < BW1; ++i)
-    for (int j = 0; j < BW1; ++j) {
-      // S_m = L_mm U_mm (forward factor), S'_m likewise from the reversed one
-      double sf = 0.0, sr = 0.0;
-      for (int k = 0; k < BW1; ++k) {
-        const double lf = (k == i) ? 1.0 : (k < i ? at(F, r0 + i, r0 + k) : 0.0);
-        const double uf = (k <= j) ? at(F, r0 + k, r0 + j) : 0.0;
-        sf += lf * uf;
-        const int ir = BW1 - 1 - i, jr = BW1 - 1 - j;
-        const double lr = (k == ir) ? 1.0 : (k < ir ? at(Fr, q0 + ir, q0 + k) : 0.0);
-        const double ur = (k <= jr) ? at(Fr, q0 + k, q0 + jr) : 0.0;
-        sr += lr * ur;
-      }
-      // D_m: the block of I + scale A, formed as the factor kernel forms it
-      double d = at(a_host, r0 + i, r0 + j) * scale;
-      if (i == j) d += 1.0;
-      P[(size_t)i * BW1 + j] = sf + sr - d;
-      // couplings: the forward factor's L of element m on element m-1, and
-      // the reversed factor's on its element mr-1 (element m+1), reversed back
-      CT[(size_t)i * BW1 + j] = at(F, r0 + i, r0 - BW1 + j);
-      CB[(size_t)i * BW1 + j] = at(Fr, q0 + (BW1 - 1 - i), q0 - BW1 + (BW1 - 1 - j));
-    }
-  // P^-1 by Gauss-Jordan elimination with partial pivoting
-  std::vector<double> Pi((size_t)BW1 * BW1, 0.0), W = P;
-  for (int i = 0; i < BW1; ++i) Pi[(size_t)i * BW1 + i] = 1.0;
-  for (int c = 0; c < BW1; ++c) {
-    int piv = c;
-    for (int r = c + 1; r < BW1; ++r)
-      if (std::fabs(W[(size_t)r * BW1 + c]) > std::fabs(W[(size_t)piv * BW1 + c])) piv = r;
-    if (W[(size_t)piv * BW1 + c] == 0.0 || !std::isfinite(W[(size_t)piv * BW1 + c])) return drop();
-    if (piv != c)
-      for (int k = 0; k < BW1; ++k) {
-        std::swap(W[(size_t)c * BW1 + k], W[(size_t)piv * BW1 + k]);
-        std::swap(Pi[(size_t)c * BW1 + k], Pi[(size_t)piv * BW1 + k]);
-      }
-    const double inv = 1.0 / W[(size_t)c * BW1 + c];
-    for (int k = 0; k < BW1; ++k) {
-      W[(size_t)c * BW1 + k] *= inv;
-      Pi[(size_t)c * BW1 + k] *= inv;
-    }
-    for (int r = 0; r < BW1; ++r)
-      if (r != c) {
-        const double f = W[(size_t)r * BW1 + c];
-        if (f != 0.0)
-          for (int k = 0; k < BW1; ++k) {
-            W[(size_t)r * BW1 + k] -= f * W[(size_t)c * BW1 + k];
-            Pi[(size_t)r * BW1 + k] -= f * Pi[(size_t)c * BW1 + k];
-          }
-      }
-  }
-  std::vector<double> GT((size_t)BW1 * BW1), GB((size_t)BW1 * BW1);
-  for (int i = 0; i < BW1; ++i)
-    for (int j = 0; j < BW1; ++j) {
-      double gt = 0.0, gb = 0.0;
-      for (int k = 0; k < BW1; ++k) {
-        gt += Pi[(size_t)i * BW1 + k] * CT[(size_t)k * BW1 + j];
-        gb += Pi[(size_t)i * BW1 + k] * CB[(size_t)k * BW1 + j];
-      }
-      GT[(size_t)i * BW1 + j] = -gt;
-      GB[(size_t)i * BW1 + j] = -gb;
-    }
-  std::vector<double> tiles(twist_mid_doubles(BW1, NS));
-  if (!twist_mid_tiles(Pi.data(), GT.data(), GB.data(), BW1, NS, tiles.data())) return drop();
-  if ((rc = dalloc(&s->fragf, frag_doubles(KV, BW1, NS)))) return rc;
-  launch_frag_prep(s->blkf, KV, BW1, NS, s->fragf, st);
-  if ((rc = dalloc(&s->fragm, tiles.size()))) return rc;
-  CK(cudaMemcpyAsync(s->fragm, tiles.data(), tiles.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-  if ((rc = dalloc(&s->rmid, (size_t)M.nlines * (BW1 + 2 * NS)))) return rc;
-  CK(cudaStreamSynchronize(st));
-  s->mid = m;
-  return check_launch("twisted solve setup");
 }
 
 int build_band(atb_solver* s, cudaStream_t st) {
@@ -1180,9 +1049,6 @@ int build_band(atb_solver* s, cudaStream_t st) {
     LineMap M1 = M;
     M1.nlines = 1;  // band1 holds one line
     launch_band_compact(M1, band1, one, st);
-    // the unfactored band, for the twisted solve's reversed factor and middle block
-    std::vector<double> a_host((size_t)M.nunk * rs);
-    CK(cudaMemcpyAsync(a_host.data(), one, a_host.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     launch_band_factor(M.nunk, M.bw, 1, one, (int)rs, 1, scale, st);
     CK(cudaStreamSynchronize(st));
     cudaFree(band1);
@@ -1202,12 +1068,6 @@ int build_band(atb_solver* s, cudaStream_t st) {
     if (!(dense && dense[0] == '1') && warp_solve_structure_ok(hblk.data(), M.KV, BW1, M.ns)) {
       if ((rc = dalloc(&s->frag, frag_doubles(M.KV, BW1, M.ns)))) return rc;
       launch_frag_prep(s->blk, M.KV, BW1, M.ns, s->frag, st);
-      // the twisted solve (ATB_BAND_TWIST=0 keeps the whole-column sweep)
-      const char* tw = std::getenv("ATB_BAND_TWIST");
-      if (!(tw && tw[0] == '0') && M.KV >= 4 && (M.ns == 4 || M.ns == 5)) {
-        CK(cudaStreamSynchronize(st));
-        if ((rc = build_twist(s, a_host, scale, st))) return rc;
-      }
     }
     CK(cudaStreamSynchronize(st));
   } else if (!rc) {
@@ -1490,10 +1350,6 @@ int ark_step_accumulated(atb_solver* s, double* const* q, cudaStream_t st) {
     B.band = s->band;
     B.blk = s->blk;
     B.frag = s->frag;
-    B.fragf = s->fragf;
-    B.fragm = s->fragm;
-    B.rmid = s->rmid;
-    B.mid = s->mid;
     B.ld = s->ld;
     B.npairs = 0;
     B.dt = s->dt;
@@ -1583,10 +1439,6 @@ int ark_step(atb_solver* s, double* const* q, cudaStream_t st) {
       B.band = s->band;
       B.blk = s->blk;
       B.frag = s->frag;
-    B.fragf = s->fragf;
-    B.fragm = s->fragm;
-    B.rmid = s->rmid;
-    B.mid = s->mid;
       B.ld = s->ld;
       B.npairs = i;
       B.dt = s->dt;

@@ -875,276 +875,6 @@ __global__ void __launch_bounds__(32 * NW) band_solve_warp_kernel(const BandSolv
   cp_async_wait<0>();
 }
 
-// ------------------------------------------------------------ twisted solve
-// The same block recurrence run from both ends of each column towards a
-// middle element m = B.mid ("burn at both ends"): the top half (elements
-// 0..m-1) is the forward sweep of the column's own factor; the bottom half
-// (elements KV-1..m+1) is the forward sweep of the factor of the column read
-// backwards (unknowns and elements reversed: the reversed matrix keeps the
-// band and the face-node coupling, so the same tiles apply).  The middle
-// element then solves P x_m = r_m - C_top y_{m-1} - C_bot z_{m+1}, P = S_m +
-// S'_m - D_m (the two sweeps' Schur complements minus the diagonal block they
-// share), and each half substitutes backwards away from it.  At KV = 16 the
-// 32 dependent element steps become 8 + 1 + 8, with twice the warps at work.
-//   PH = 0: the forward sweeps; CTAs [0, G) the top half, [G, 2G) the bottom
-//           half (reversed); the top half also saves r_m into B.rmid (the
-//           solve runs in place, and element m's values are overwritten only
-//           in phase 1)
-//   PH = 1: each half solves the middle element from B.rmid and the two
-//           sweeps' results next to it, then its backward sweep; the top half
-//           writes x_m
-template <int NQ, int NS, int NW, int PH>
-__global__ void __launch_bounds__(32 * NW) band_solve_twist_kernel(const BandSolve B, int G) {
-  constexpr int BW1 = NQ * NS;
-  using S = WarpSolveShape<BW1, NS>;
-  constexpr int MT = S::MT, KT = S::KT, KP = S::KP, RW = S::RW, LD = S::LD, FR = S::FR, RS = S::RS;
-  constexpr int T0 = S::T0, T1 = S::T1;
-  constexpr int JT = (BW1 + 3) / 4;
-  extern __shared__ __align__(16) double sm[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = lane >> 2, tq = lane & 3;
-  const int role = (int)blockIdx.x >= G ? 1 : 0;  // 0: top half, 1: bottom half (reversed)
-  const int cta = (int)blockIdx.x - role * G;
-  double* Fr = sm;                               // [RS][FR], shared by the CTA's warps
-  double* ring = sm + RS * FR + warp * S::WBUF;  // [RS][KP][LD]: right-hand sides
-  double* Wb = ring + RS * KP * LD;              // [2][RW][LD]: results of the last two elements
-  const LineMap& M = B.M;
-  const int KV = M.KV, nh = M.nh, Np = M.Np, m = B.mid;
-  const int KVh = role ? KV - 1 - m : m;  // elements of this half
-  const size_t lstep = (size_t)M.estep * Np;
-  const double* frag = role ? B.fragf : B.frag;
-  const int line0 = (cta * NW + warp) * 8;
-  // element ev of this half -> offset of its original element in the fields
-  auto eoff = [&](int ev) -> size_t { return (size_t)(role ? KV - 1 - ev : ev) * lstep; };
-  // row r of an element of this half -> original row (reversed in the bottom half)
-  auto orow = [&](int r) { return role ? BW1 - 1 - r : r; };
-  for (int i = lane; i < S::WBUF; i += 32) ring[i] = 0.0;
-  // ---- RHS loader: lane owns line (lane & 7) and rows 4j + (lane >> 3)
-  const int ll = lane & 7;
-  const bool lact = line0 + ll < M.nlines;
-  const size_t lb = lact ? (size_t)M.e0[line0 + ll] * Np + (line0 + ll) % nh : 0;
-  size_t roff[JT];
-  int rsel[JT];
-#pragma unroll
-  for (int j = 0; j < JT; ++j) {
-    const int row = 4 * j + (lane >> 3);
-    const int ro = row < BW1 ? orow(row) : 0;
-    rsel[j] = (lact && row < BW1) ? ro % NS : -1;
-    roff[j] = lb + (row < BW1 ? (size_t)nh * (ro / NS) : 0);
-  }
-  auto field = [&](auto f, int s) {
-    auto p = f[0];
-#pragma unroll
-    for (int c = 1; c < NS; ++c)
-      if (c == s) p = f[c];
-    return p;
-  };
-  // forward: the right-hand side; backward: the forward results (in place)
-  const double* src[JT];
-#pragma unroll
-  for (int j = 0; j < JT; ++j) {
-    const int sj = rsel[j] < 0 ? 0 : rsel[j];
-    src[j] = (PH == 0 ? (const double*)field(B.q, sj) : (const double*)field(B.out, sj)) + roff[j];
-  }
-  // ---- outputs: rows 8 mt + g of this half's order, lines 2 tq + i
-  double* dst[MT][2];
-#pragma unroll
-  for (int i = 0; i < 2; ++i) {
-    const int line = line0 + 2 * tq + i;
-    const bool act = line < M.nlines;
-    const size_t ob = act ? (size_t)M.e0[line] * Np + line % nh : 0;
-#pragma unroll
-    for (int mt = 0; mt < MT; ++mt) {
-      const int row = 8 * mt + g;
-      const int ro = row < BW1 ? orow(row) : 0;
-      dst[mt][i] = (act && row < BW1) ? field(B.out, ro % NS) + (size_t)nh * (ro / NS) + ob : nullptr;
-    }
-  }
-  auto issue = [&](auto passc, int ev, int slot) {
-    constexpr int P = decltype(passc)::value;
-    if (ev >= 0 && ev < KVh) {
-      const size_t evoff = eoff(ev);
-      constexpr int n16 = (P ? T1 : T0) * 16;
-      const double* gf = frag + ((size_t)ev * (T0 + T1) + (P ? T0 : 0)) * 32 + 2 * threadIdx.x;
-      double* sf = Fr + slot * FR + 2 * threadIdx.x;
-#pragma unroll
-      for (int c = 0; c < n16; c += 32 * NW)
-        if (c + (int)threadIdx.x < n16) cp_async16g(sf + 2 * c, gf + 2 * c);
-      double* sr = ring + slot * KP * LD + (lane >> 3) * LD + ll;
-#pragma unroll
-      for (int j = 0; j < JT; ++j)
-        if (rsel[j] >= 0) cp_async8(sr + 4 * j * LD, src[j] + evoff);
-    }
-    cp_async_commit();
-  };
-  auto step = [&](auto passc, int slot, int ev, int par) {
-    constexpr int P = decltype(passc)::value;
-    const size_t evoff = eoff(ev);
-    const double* F = Fr + slot * FR + lane;
-    const double* V = ring + slot * KP * LD;
-    const double* Wp = Wb + (par ^ 1) * RW * LD;
-    double* Wn = Wb + par * RW * LD;
-    constexpr TileRange cr = tile_range(BW1, NS, P, 1, 0);
-    double bv[KT], bw[KT];
-#pragma unroll
-    for (int kt = 0; kt < KT; ++kt) {
-      bv[kt] = V[(4 * kt + tq) * LD + g];
-      bw[kt] = (kt >= cr.lo && kt <= cr.hi) ? Wp[(4 * kt + tq) * LD + g] : 0.0;
-    }
-    double aA[MT][2], aC[MT][2];
-#pragma unroll
-    for (int mt = 0; mt < MT; ++mt) aA[mt][0] = aA[mt][1] = aC[mt][0] = aC[mt][1] = 0.0;
-    static_for<KT>([&](auto ktc) {
-      constexpr int kt = decltype(ktc)::value;
-      static_for<MT>([&](auto mtc) {
-        constexpr int mt = decltype(mtc)::value;
-        constexpr TileRange rc = tile_range(BW1, NS, P, 1, mt);
-        if constexpr (kt >= rc.lo && kt <= rc.hi) {
-          constexpr int off = (tile_off(BW1, NS, P, 1, mt) + kt - rc.lo) * 32;
-          dmma_8x8x4(aC[mt][0], aC[mt][1], F[off], bw[kt]);
-        }
-      });
-    });
-    static_for<KT>([&](auto ktc) {
-      constexpr int kt = decltype(ktc)::value;
-      static_for<MT>([&](auto mtc) {
-        constexpr int mt = decltype(mtc)::value;
-        constexpr TileRange ra = tile_range(BW1, NS, P, 0, mt);
-        if constexpr (kt >= ra.lo && kt <= ra.hi) {
-          constexpr int off = (tile_off(BW1, NS, P, 0, mt) + kt - ra.lo) * 32;
-          dmma_8x8x4(aA[mt][0], aA[mt][1], F[off], bv[kt]);
-        }
-      });
-    });
-#pragma unroll
-    for (int mt = 0; mt < MT; ++mt) {
-      const int row = 8 * mt + g;
-      const double y0 = aA[mt][0] + aC[mt][0], y1 = aA[mt][1] + aC[mt][1];
-      *reinterpret_cast<double2*>(Wn + row * LD + 2 * tq) = make_double2(y0, y1);
-      if (dst[mt][0]) dst[mt][0][evoff] = y0;
-      if (dst[mt][1]) dst[mt][1][evoff] = y1;
-    }
-  };
-  const std::integral_constant<int, 0> fwd{};
-  const std::integral_constant<int, 1> bwd{};
-  __syncthreads();
-  if constexpr (PH == 0) {
-    // ---- the middle element's right-hand side, saved before any solve
-    // writes in place ([line][row], original row order)
-    if (role == 0 && lact) {
-      const size_t mo = (size_t)m * lstep;
-#pragma unroll
-      for (int j = 0; j < JT; ++j)
-        if (rsel[j] >= 0) B.rmid[(size_t)(line0 + ll) * (BW1 + 2 * NS) + 4 * j + (lane >> 3)] = src[j][mo];
-    }
-    // ---- forward sweep of this half
-    issue(fwd, 0, 0);
-    issue(fwd, 1, 1);
-    int slot = 0;
-    for (int ev = 0; ev < KVh; ++ev) {
-      cp_async_wait<1>();
-      __syncthreads();  // element ev in place; every warp is past element ev-1
-      step(fwd, slot, ev, ev & 1);
-      issue(fwd, ev + 2, slot == 0 ? RS - 1 : slot - 1);
-      slot = slot == RS - 1 ? 0 : slot + 1;
-    }
-    cp_async_wait<0>();
-    // the last NS rows (this half's order) of the sweep's result next to the
-    // middle -- what the middle element couples to -- saved beside r_m: the
-    // other half overwrites them in place during its backward sweep
-    __syncwarp();
-    const double* Wl = Wb + ((KVh - 1) & 1) * RW * LD;
-    for (int t = lane; t < 8 * NS; t += 32) {
-      const int l = t / NS, k = t - l * NS;
-      if (line0 + l < M.nlines)
-        B.rmid[(size_t)(line0 + l) * (BW1 + 2 * NS) + BW1 + role * NS + k] = Wl[(BW1 - NS + k) * LD + l];
-    }
-  } else {
-    // ---- middle element: x_m = P^-1 r_m - (P^-1 C_top) y_{m-1} - (P^-1 C_bot) z_{m+1},
-    // the three right-hand vectors staged [row][line] in ring slots 0..2
-    double* Vm = ring;
-    double* Ym = ring + KP * LD;
-    double* Zm = ring + 2 * KP * LD;
-    const double* rm = B.rmid + (size_t)(line0 + ll) * (BW1 + 2 * NS);
-#pragma unroll
-    for (int j = 0; j < JT; ++j) {
-      const int row = 4 * j + (lane >> 3);
-      if (lact && row < BW1) Vm[row * LD + ll] = rm[row];
-    }
-    // y_{m-1}: its last NS rows; z_{m+1} (stored reversed by the bottom
-    // half): its first NS rows; every other row stays zero
-    if (lact && (lane >> 3) == 0) {
-#pragma unroll
-      for (int k = 0; k < NS; ++k) {
-        Ym[(BW1 - NS + k) * LD + ll] = rm[BW1 + k];
-        Zm[(NS - 1 - k) * LD + ll] = rm[BW1 + NS + k];
-      }
-    }
-    __syncwarp();
-    constexpr int KTL = (BW1 - NS) / 4;  // first k-tile holding the last NS columns
-    constexpr int KTF = (NS - 1) / 4;    // last k-tile holding the first NS columns
-    constexpr int OFF_T = MT * KT, OFF_B = OFF_T + MT * (KT - KTL);
-    const double* Fm = B.fragm + lane;
-    double x[MT][2];
-#pragma unroll
-    for (int mt = 0; mt < MT; ++mt) x[mt][0] = x[mt][1] = 0.0;
-    static_for<KT>([&](auto ktc) {
-      constexpr int kt = decltype(ktc)::value;
-      const double b = Vm[(4 * kt + tq) * LD + g];
-      static_for<MT>([&](auto mtc) {
-        constexpr int mt = decltype(mtc)::value;
-        dmma_8x8x4(x[mt][0], x[mt][1], __ldg(Fm + (mt * KT + kt) * 32), b);
-      });
-    });
-    static_for<KT - KTL>([&](auto kc) {
-      constexpr int k = decltype(kc)::value;
-      const double b = Ym[(4 * (KTL + k) + tq) * LD + g];
-      static_for<MT>([&](auto mtc) {
-        constexpr int mt = decltype(mtc)::value;
-        dmma_8x8x4(x[mt][0], x[mt][1], __ldg(Fm + (OFF_T + mt * (KT - KTL) + k) * 32), b);
-      });
-    });
-    static_for<KTF + 1>([&](auto kc) {
-      constexpr int k = decltype(kc)::value;
-      const double b = Zm[(4 * k + tq) * LD + g];
-      static_for<MT>([&](auto mtc) {
-        constexpr int mt = decltype(mtc)::value;
-        dmma_8x8x4(x[mt][0], x[mt][1], __ldg(Fm + (OFF_B + mt * (KTF + 1) + k) * 32), b);
-      });
-    });
-    // x_m: the coupling input of this half's first backward step (in this
-    // half's row order), and the solution of element m (top half writes it)
-    double* W0 = Wb + ((KVh & 1) ^ 1) * RW * LD;
-#pragma unroll
-    for (int mt = 0; mt < MT; ++mt) {
-      const int row = 8 * mt + g;
-      if (row < BW1) {
-        const int r = orow(row);
-        W0[r * LD + 2 * tq] = x[mt][0];
-        W0[r * LD + 2 * tq + 1] = x[mt][1];
-        if (role == 0) {
-          if (dst[mt][0]) dst[mt][0][(size_t)m * lstep] = x[mt][0];
-          if (dst[mt][1]) dst[mt][1][(size_t)m * lstep] = x[mt][1];
-        }
-      }
-    }
-    __syncwarp();  // ring slots 0..2 are refilled below
-    // ---- backward sweep of this half, from its element next to the middle
-    issue(bwd, KVh - 1, 0);
-    issue(bwd, KVh - 2, 1);
-    int slot = 0;
-    for (int t = 0; t < KVh; ++t) {
-      const int ev = KVh - 1 - t;
-      cp_async_wait<1>();
-      __syncthreads();
-      step(bwd, slot, ev, (KVh + t) & 1);
-      issue(bwd, ev - 2, slot == 0 ? RS - 1 : slot - 1);
-      slot = slot == RS - 1 ? 0 : slot + 1;
-    }
-    cp_async_wait<0>();
-  }
-}
-
 template <int NQ, int NS, int NW>
 constexpr size_t warp_solve_smem() {
   using S = WarpSolveShape<NQ * NS, NS>;
@@ -1278,111 +1008,10 @@ bool warp_solve_structure_ok(const double* blk_host, int KV, int BW1, int NS) {
 }
 
 
-__global__ void band_reverse_kernel(const double* band, int n, int bw, double* out) {
-  const int rs = 2 * (bw + 1);
-  const size_t total = (size_t)n * rs;
-  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
-    const size_t i = t / rs;
-    const int o = (int)(t - i * rs);  // offset j - i + bw of entry (i, j)
-    out[t] = (o <= 2 * bw) ? band[((size_t)n - 1 - i) * rs + (2 * bw - o)] : 0.0;
-  }
-}
-
-void launch_band_reverse(const double* band, int n, int bw, double* out, cudaStream_t st) {
-  const size_t total = (size_t)n * 2 * (bw + 1);
-  band_reverse_kernel<<<(int)((total + 255) / 256 < 1024 ? (total + 255) / 256 : 1024), 256, 0, st>>>(band, n, bw,
-                                                                                                        out);
-}
-
-size_t twist_mid_doubles(int BW1, int NS) {
-  const int MT = (BW1 + 7) / 8, KT = (BW1 + 3) / 4, KTL = (BW1 - NS) / 4, KTF = (NS - 1) / 4;
-  return (size_t)32 * MT * (KT + (KT - KTL) + (KTF + 1));
-}
-
-bool twist_mid_tiles(const double* Pi, const double* GT, const double* GB, int BW1, int NS, double* tiles) {
-  const int MT = (BW1 + 7) / 8, KT = (BW1 + 3) / 4, KTL = (BW1 - NS) / 4, KTF = (NS - 1) / 4;
-  for (int i = 0; i < BW1; ++i)
-    for (int j = 0; j < BW1; ++j) {
-      if (j < 4 * KTL && GT[i * BW1 + j] != 0.0) return false;
-      if (j > 4 * KTF + 3 && GB[i * BW1 + j] != 0.0) return false;
-    }
-  // tile (mt, kt), lane l: M[8 mt + l / 4][4 kt + l % 4] (zero outside BW1 x BW1)
-  auto put = [&](const double* Mx, int mt, int kt, double* t) {
-    for (int l = 0; l < 32; ++l) {
-      const int r = 8 * mt + l / 4, c = 4 * kt + l % 4;
-      t[l] = (r < BW1 && c < BW1) ? Mx[r * BW1 + c] : 0.0;
-    }
-  };
-  double* t = tiles;
-  for (int mt = 0; mt < MT; ++mt)
-    for (int kt = 0; kt < KT; ++kt, t += 32) put(Pi, mt, kt, t);
-  for (int mt = 0; mt < MT; ++mt)
-    for (int kt = KTL; kt < KT; ++kt, t += 32) put(GT, mt, kt, t);
-  for (int mt = 0; mt < MT; ++mt)
-    for (int kt = 0; kt <= KTF; ++kt, t += 32) put(GB, mt, kt, t);
-  return true;
-}
-
-template <int NQ, int NS, int NW>
-void twist_launch_nw(const BandSolve& B, cudaStream_t st) {
-  constexpr size_t smem = warp_solve_smem<NQ, NS, NW>();
-  static bool configured = false;
-  if (!configured && smem > 48 * 1024) {
-    cudaFuncSetAttribute(band_solve_twist_kernel<NQ, NS, NW, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
-    cudaFuncSetAttribute(band_solve_twist_kernel<NQ, NS, NW, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
-  }
-  configured = true;
-  const int warps = (B.M.nlines + 7) / 8;
-  const int G = (warps + NW - 1) / NW;  // CTAs per half
-  band_solve_twist_kernel<NQ, NS, NW, 0><<<2 * G, 32 * NW, smem, st>>>(B, G);
-  band_solve_twist_kernel<NQ, NS, NW, 1><<<2 * G, 32 * NW, smem, st>>>(B, G);
-}
-
-template <int NQ, int NS>
-bool twist_launch(const BandSolve& B, cudaStream_t st) {
-  static int nsm = 0;
-  if (!nsm) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (nsm <= 0) nsm = 148;
-  }
-  const size_t smem[4] = {warp_solve_smem<NQ, NS, 2>(), warp_solve_smem<NQ, NS, 3>(), warp_solve_smem<NQ, NS, 4>(),
-                          warp_solve_smem<NQ, NS, 6>()};
-  // both halves run at once: twice the warps of the whole-column solve
-  switch (pick_nw(2 * ((B.M.nlines + 7) / 8), nsm, smem)) {
-    case 2: twist_launch_nw<NQ, NS, 2>(B, st); return true;
-    case 3: twist_launch_nw<NQ, NS, 3>(B, st); return true;
-    case 4: twist_launch_nw<NQ, NS, 4>(B, st); return true;
-    case 6: twist_launch_nw<NQ, NS, 6>(B, st); return true;
-  }
-  return false;
-}
-
-template <int NS> warp_fn pick_twist(int nq) {
-  switch (nq) {
-    case 2: return twist_launch<2, NS>;
-    case 3: return twist_launch<3, NS>;
-    case 4: return twist_launch<4, NS>;
-    case 5: return twist_launch<5, NS>;
-    case 6: return twist_launch<6, NS>;
-    case 7: return twist_launch<7, NS>;
-    case 8: return twist_launch<8, NS>;
-  }
-  return nullptr;
-}
-
-// Dispatch: the twisted block-parallel form when its tiles were prepared,
-// else the whole-column block-parallel form when the factor is shared and its
+// Dispatch: the block-parallel form when the factor is shared and its
 // per-element inverses were prepared, else the register-window substitution
 // (shared factor), else the generic per-line kernel.
 void launch_band_solve(const BandSolve& B, cudaStream_t st) {
-  if (B.ld == 1 && B.frag && B.fragf && B.fragm && B.rmid && B.npairs == 0 && (B.M.ns == 4 || B.M.ns == 5)) {
-    warp_fn w = B.M.ns == 4 ? pick_twist<4>(B.M.Nq) : pick_twist<5>(B.M.Nq);
-    if (w && w(B, st)) return;
-  }
   if (B.ld == 1 && B.frag && B.npairs == 0 && (B.M.ns == 4 || B.M.ns == 5)) {
     warp_fn w = B.M.ns == 4 ? pick_warp<4>(B.M.Nq) : pick_warp<5>(B.M.Nq);
     if (w && w(B, st)) return;

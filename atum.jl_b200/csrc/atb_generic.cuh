@@ -71,15 +71,6 @@ struct BandSolve {
   double* out[5];
   const double* blk;  // per-element [L^-1 | G | U^-1 | H] blocks (shared factor), or null
   const double* frag; // the same blocks in matrix-unit fragment order (launch_frag_prep), or null
-  // twisted solve (both ends towards the middle element mid): the tiles of the
-  // reversed column's factor, the middle element's tiles [P^-1 | -P^-1 C_top |
-  // -P^-1 C_bottom] (launch_twist_prep), and a buffer per line for the middle
-  // element's right-hand side and the two sweeps' coupling rows
-  // (nlines x (BW1 + 2 ns)); fragf null: no twisted solve
-  const double* fragf;
-  const double* fragm;
-  double* rmid;
-  int mid;
 };
 void launch_band_solve(const BandSolve& B, cudaStream_t st);
 void launch_block_prep(const double* band, int KV, int BW1, double* blk, cudaStream_t st);
@@ -88,15 +79,6 @@ size_t frag_doubles(int KV, int BW1, int NS);
 void launch_frag_prep(const double* blk, int KV, int BW1, int NS, double* frag, cudaStream_t st);
 // whether the blocks (host copy of blk) have the zero structure those tiles assume
 bool warp_solve_structure_ok(const double* blk_host, int KV, int BW1, int NS);
-// the reversed column's compact band (row stride 2*(bw+1)): entry (i, j) of
-// the output is entry (n-1-i, n-1-j) of the input
-void launch_band_reverse(const double* band, int n, int bw, double* out, cudaStream_t st);
-// doubles of the middle element's tiles of the twisted solve
-size_t twist_mid_doubles(int BW1, int NS);
-// middle element's tiles from the host matrices P^-1, -P^-1 C_top (nonzero in
-// the last NS columns) and -P^-1 C_bottom (nonzero in the first NS columns),
-// BW1 x BW1 row-major each; false when the couplings leave those columns
-bool twist_mid_tiles(const double* Pi, const double* GT, const double* GB, int BW1, int NS, double* tiles);
 
 void launch_red_finish(const double* partials, int nblocks, int linf, double* out5, cudaStream_t st);
 double probe_fp64_tflops(cudaStream_t st);

@@ -841,15 +841,6 @@ typedef void (*tend_launch_fn)(const TendArgs& A, int grid, int block, size_t sm
 template <int LAW, int DIM, int VK, int NQ_ = 0, bool FUSE = false, int SF = -1>
 void tend_launch(const TendArgs& A, int grid, int block, size_t smem, cudaStream_t st) {
   static size_t configured = 0;
-  static bool carveout = false;
-  if (FUSE && !carveout) {
-    // the fused stage kernels are occupancy-limited by shared memory: ask for
-    // the largest carveout (a hint; the launch does not depend on it)
-    cudaFuncSetAttribute(tendency_kernel<LAW, DIM, VK, NQ_, FUSE, SF>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         100);
-    cudaGetLastError();
-    carveout = true;
-  }
   if (smem > 48 * 1024 && smem > configured) {
     // on failure the launch below reports the error
     if (cudaFuncSetAttribute(tendency_kernel<LAW, DIM, VK, NQ_, FUSE, SF>, cudaFuncAttributeMaxDynamicSharedMemorySize,

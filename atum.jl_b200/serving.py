@@ -281,7 +281,8 @@ class _Pool:
         self.inflight = []       # (event, [(request, pinned view)], buffer) per tick
         self.inflight_prefix = 0
         self.naux = template.descriptor_fields()["naux"]
-        self.host = {"dt": 0.0, "launch": 0.0, "results": 0.0, "compact": 0.0}
+        self.host = {"dt": 0.0, "launch": 0.0, "results": 0.0, "compact": 0.0, "admit_make": 0.0,
+                     "admit_place": 0.0}
 
     # a Solver binds to a pool as to an operator
     @property
@@ -336,15 +337,20 @@ class _Pool:
             if r.make is None:
                 # the caller's tensors were written on its current stream
                 self.copy_stream.wait_stream(torch.cuda.current_stream())
+            t0 = time.perf_counter()
             with torch.cuda.stream(self.copy_stream):
                 if r.make is not None:
                     q0, aux = r.make()
                 else:
                     q0 = r.q0
                     aux = r.aux if isinstance(r.aux, torch.Tensor) else None
+                t1 = time.perf_counter()
                 self._place(p, self.copy_stream, aux=aux.reshape(-1) if aux is not None else None)
+                t2 = time.perf_counter()
                 self.q[:, p.first:p.first + K].copy_(q0.reshape(self.ns, K, self.Np), non_blocking=True)
                 ev = self.copy_stream.record_event()
+            self.host["admit_make"] += t1 - t0
+            self.host["admit_place"] += t2 - t1
             self.pending.append(ev)
             self.placed.append(p)
             self.used = p.first + K

@@ -599,11 +599,13 @@ def run_serve(args):
     srv.run(warm, realtime=False)
     with ClockSampler(torch.cuda.current_device()) as clk:
         st = srv.run(reqs, realtime=True)
+    clocks = clk.summary()  # read before the next sampler reuses the file
     # the same arrivals with end times a fifth as long: an offered load one
     # B200 sustains, so latency measures serving rather than queueing
     reqs_s, _ = stream(args.time_scale / 5, 20261203 + rank)
     with ClockSampler(torch.cuda.current_device()) as clk_s:
         st_s = srv.run(reqs_s, realtime=True)
+    clocks_s = clk_s.summary()
     lat_s = np.array([r.latency for r in reqs_s])
     # accuracy: a sample of requests stepped alone in FP64 from the same
     # device-built initial state
@@ -642,7 +644,7 @@ def run_serve(args):
                                       "mean": st_s.mean_latency_s, "max": float(lat_s.max())},
                         "makespan_s": st_s.makespan_s, "arrival_window_s": max(r.arrival for r in reqs_s),
                         "dof_stage_updates": st_s.extra["dof_stage_updates"],
-                        "host_seconds": st_s.extra["host_seconds"], "clocks": clk_s.summary()},
+                        "host_seconds": st_s.extra["host_seconds"], "clocks": clocks_s},
         "inputs": "built on the device at admission (grid points, aux fields, initial state)",
         "results": "per-component weighted L2 norms copied back; whole states only for the sampled requests",
         "makespan_s": st.makespan_s, "arrival_window_s": max(r.arrival for r in reqs),
@@ -652,7 +654,7 @@ def run_serve(args):
         "peak_pool_bytes": st.peak_pool_bytes, "dof_stage_updates": st.extra["dof_stage_updates"],
         "rel_l2_vs_fp64": {"samples": len(errs), "max": max(errs) if errs else None,
                            "median": float(np.median(errs)) if errs else None},
-        "clocks": clk.summary(),
+        "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
     if dist is not None:

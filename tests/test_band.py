@@ -13,12 +13,11 @@ import problems as P
 pytestmark = pytest.mark.gpu
 
 
-def _ark_run(case, steps, monkeypatch, dense, twist=False):
+def _ark_run(case, steps, monkeypatch, dense):
     if dense:
         monkeypatch.setenv("ATB_BAND_DENSE", "1")
     else:
         monkeypatch.delenv("ATB_BAND_DENSE", raising=False)
-    monkeypatch.setenv("ATB_BAND_TWIST", "1" if twist else "0")
     q = PT.to_dev(case.q0)
     s = A.ARK23(case.dg, case.lindg, q, case.dt, split_rhs=False)
     s.step(q, steps)
@@ -34,23 +33,6 @@ def test_warp_band_solve_bitwise_equals_dense(N, K, monkeypatch):
     b = _ark_run(case, 3, monkeypatch, dense=True)
     assert np.isfinite(a).all()
     assert np.array_equal(a, b)
-
-
-@pytest.mark.parametrize("N,K", [(1, (3, 3, 4)), (2, (3, 2, 5)), (3, 4), (4, (2, 3, 6)), (4, 16), (5, (2, 2, 7)),
-                                 (6, (2, 2, 4)), (7, (2, 2, 8))])
-def test_twisted_band_solve_equals_whole_column(N, K, monkeypatch):
-    """The solve from both ends of each column towards its middle element
-    (band_solve_twist_kernel, the default for four or more elements per
-    column) against the whole-column sweep over whole ARK23 runs: equal to
-    1e-13 relative per component (the same elimination, other pivot blocks),
-    for even and odd column heights and every order."""
-    case = P.bubble_3d(N=N, K=K, imex=True, steps=3)
-    a = _ark_run(case, 3, monkeypatch, dense=False, twist=True)
-    b = _ark_run(case, 3, monkeypatch, dense=False, twist=False)
-    assert np.isfinite(a).all()
-    err = PT.field_rel_errors(a, b)
-    assert np.all(err <= 1e-13), err
-    assert not np.array_equal(a, b)  # the twisted kernel ran
 
 
 def test_warp_band_solve_stacked_columns_vs_oracle(monkeypatch):
