@@ -676,9 +676,21 @@ class Server:
                 nxt += 1
             waiting = []
             ta = time.perf_counter()
-            for r in queue:  # FIFO admission
+            # FIFO admission; once a request of a kind found no room in this
+            # pass, requests of that kind at least as large wait without
+            # another search (under overload the queue is long)
+            blocked: Dict[tuple, int] = {}
+            for r in queue:
+                key = self._keys.get(id(r.dg))
+                if key is None:
+                    key = self._keys[id(r.dg)] = kind_key(r.dg)
+                K = r.dg.grid.K
+                if key in blocked and K >= blocked[key]:
+                    waiting.append(r)
+                    continue
                 p = self._find_pool(r)
                 if p is None:
+                    blocked[key] = min(K, blocked.get(key, K))
                     waiting.append(r)
                 else:
                     p.admit(r, now())
