@@ -463,6 +463,10 @@ int op_create_impl(const atb_op_desc* descs, int n, const double* const* aux_hos
   }
   if (!fn) return fail(ATB_ERR_INVALID, "unsupported (law %d, volume flux %d) combination", d->law, d->volume_flux);
   const int sf = d->surface_flux;
+  if (sf == ATB_FLUX_RUSANOV) {
+    // the kernel with the surface flux built in, where one is compiled
+    if (tend_launch_fn fr = pick_launcher_rusanov(d->law, d->dim, vk, nq)) fn = fr;
+  }
   bool sf_ok = sf == ATB_FLUX_CENTRAL || sf == ATB_FLUX_RUSANOV;
   if (d->law == LAW_EULER || d->law == LAW_EG) sf_ok = sf_ok || (sf >= ATB_FLUX_EC && sf <= ATB_FLUX_MATRIX);
   if (d->law == LAW_SW) sf_ok = sf_ok || sf == ATB_FLUX_EC || sf == ATB_FLUX_ROE;

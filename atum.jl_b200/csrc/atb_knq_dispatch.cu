@@ -15,6 +15,21 @@ tend_launch_fn pick_nq_leg_2_vk_weak(int nq);
 tend_launch_fn pick_nq_euler_2_vk_ec(int nq);
 tend_launch_fn pick_nq_euler_3_vk_ec(int nq);
 tend_launch_fn pick_nq_sw_2_vk_ec(int nq);
+tend_launch_fn pick_rus_eg_3_ec(int nq);
+tend_launch_fn pick_rus_eg_3_ec32(int nq);
+tend_launch_fn pick_rus_euler_2_ec(int nq);
+tend_launch_fn pick_rus_euler_2_ec32(int nq);
+tend_launch_fn pick_rus_sw_2_ec(int nq);
+tend_launch_fn pick_rus_sw_2_ec32(int nq);
+tend_launch_fn pick_launcher_rusanov(int law, int dim, int vk, int nq) {
+  if (law == LAW_EG && dim == 3 && vk == VK_EC) return pick_rus_eg_3_ec(nq);
+  if (law == LAW_EG && dim == 3 && vk == VK_EC32) return pick_rus_eg_3_ec32(nq);
+  if (law == LAW_EULER && dim == 2 && vk == VK_EC) return pick_rus_euler_2_ec(nq);
+  if (law == LAW_EULER && dim == 2 && vk == VK_EC32) return pick_rus_euler_2_ec32(nq);
+  if (law == LAW_SW && dim == 2 && vk == VK_EC) return pick_rus_sw_2_ec(nq);
+  if (law == LAW_SW && dim == 2 && vk == VK_EC32) return pick_rus_sw_2_ec32(nq);
+  return nullptr;
+}
 template <> tend_launch_fn pick_launcher_nq<LAW_ADV>(int dim, int vk, int nq) {
   (void)dim; (void)vk; (void)nq;
   return nullptr;

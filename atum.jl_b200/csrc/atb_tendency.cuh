@@ -859,6 +859,9 @@ tend_launch_fn pick_launcher_fused(int dim, int vk, int nq, int sflux, int lin_s
 
 // generic (runtime Nq) launcher, and the compile-time-Nq specialisations
 // that exist for (law, dim, vk, nq) -- nullptr when there is none
+// the compile-time-Nq kernels with the Rusanov surface flux built in (hot
+// explicit configurations), nullptr when there is none
+tend_launch_fn pick_launcher_rusanov(int law, int dim, int vk, int nq);
 template <int LAW> tend_launch_fn pick_launcher(int dim, int vk);
 template <int LAW> tend_launch_fn pick_launcher_nq(int dim, int vk, int nq);
 
