@@ -11,6 +11,7 @@ The directory name is not a Python identifier: load it as ``atum_b200`` with
 ``importlib`` spec over this directory; the tests do the same in conftest).
 """
 from .cell import LobattoCell, BrickGrid, brickgrid, min_node_distance, points
+from .cubedsphere import CubedSphereGrid, cubedspheregrid
 from .laws import (AbstractProblem, DummyProblem, ReflectiveWall, InflowZero, DirichletByTag, Coriolis,
                    AbstractBalanceLaw, AdvectionLaw, EulerLaw, EulerGravityLaw, LinearEulerGravityLaw,
                    ShallowWaterLaw, numberofstates, constants,

@@ -43,7 +43,25 @@ class DeviceOp:
         desc, keep = make_desc(dg)
         h = C.c_void_p()
         dev_aux = getattr(dg, "_aux_dev", None)
-        if dev_aux is not None:
+        if hasattr(dg.grid, "geometry"):
+            # curved elements: the grid's metric terms, face normals / masses and face map
+            G = dg.grid.geometry()
+            arrs = [np.ascontiguousarray(G[k], dtype=np.float64) for k in ("g", "MJ", "normals", "faceMJ")]
+            nb = np.ascontiguousarray(G["nbr_node"], dtype=np.int64)
+            bt = np.ascontiguousarray(G["btag"], dtype=np.int32)
+            geo = _lib.CurvedGeometry(_lib.dptr(arrs[0]), _lib.dptr(arrs[1]), _lib.dptr(arrs[2]), _lib.dptr(arrs[3]),
+                                      nb.ctypes.data_as(C.POINTER(C.c_longlong)),
+                                      bt.ctypes.data_as(C.POINTER(C.c_int)))
+            aux = None if dev_aux is not None else np.ascontiguousarray(dg.auxstate_host(), dtype=np.float64)
+            _lib.check(_lib.lib().atb_op_create_curved(C.byref(desc), _lib.dptr(aux) if aux is not None and aux.size
+                                                       else None, C.byref(geo), C.byref(h)))
+            self.h = h
+            if dev_aux is not None:
+                _lib.check(_lib.lib().atb_op_set_aux(h, C.cast(C.c_void_p(dev_aux.data_ptr()), _lib._DP),
+                                                     _lib.stream_ptr()))
+                import torch
+                torch.cuda.current_stream().synchronize()
+        elif dev_aux is not None:
             # aux evaluated on the device: create with zeros, then copy device to device
             _lib.check(_lib.lib().atb_op_create(C.byref(desc), None, C.byref(h)))
             self.h = h

@@ -46,6 +46,15 @@ STAGE_CB = C.CFUNCTYPE(C.c_int, C.c_double, C.c_double, C.POINTER(C.c_void_p), C
 
 # exported entry points and their argtypes (every one returns int status)
 _VP, _DP, _IP = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int)
+class CurvedGeometry(C.Structure):
+    """``atb_curved_geometry``: per-node metric terms and M J, per face node
+    normals, face masses and neighbour nodes, per face boundary tags."""
+    _fields_ = [
+        ("metric", C.POINTER(C.c_double)), ("mj", C.POINTER(C.c_double)), ("normals", C.POINTER(C.c_double)),
+        ("face_mj", C.POINTER(C.c_double)), ("nbr_node", C.POINTER(C.c_longlong)), ("btag", C.POINTER(C.c_int)),
+    ]
+
+
 SIGNATURES = {
     "atb_version": [],
     "atb_device_count": [_IP],
@@ -53,6 +62,7 @@ SIGNATURES = {
     "atb_op_destroy": [_VP],
     "atb_op_dims": [_VP, _IP, _IP, _IP],
     "atb_op_set_aux": [_VP, _DP, _VP],
+    "atb_op_create_curved": [C.POINTER(OpDesc), _DP, C.POINTER(CurvedGeometry), C.POINTER(C.c_void_p)],
     "atb_op_create_batch": [C.POINTER(OpDesc), C.c_int, C.POINTER(_DP), C.POINTER(C.c_void_p)],
     "atb_op_instances": [_VP, _IP, _IP],
     "atb_op_autotune": [_VP, PtrArr, _DP, _VP, _IP],

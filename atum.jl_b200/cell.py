@@ -242,6 +242,8 @@ def min_node_distance(grid: BrickGrid, dims=None) -> float:
     """Smallest distance between neighbouring nodes along ``dims`` (1-based)."""
     if dims is None:
         dims = range(1, grid.dim + 1)
+    if hasattr(grid, "min_node_distance"):  # curved grids measure their node coordinates
+        return grid.min_node_distance(dims)
     gap = float(np.min(np.diff(grid.cell.nodes)))
     best = math.inf
     for d in dims:

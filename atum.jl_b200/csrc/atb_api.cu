@@ -9,6 +9,7 @@
 #include "atb_generic.cuh"
 #include "atb_reduce.cuh"
 #include "atb_tendency.cuh"
+#include "atb_curved.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -170,6 +171,15 @@ struct atb_op {
   int prof_class = ATB_PROF_TEND;
   int E = 1;
   size_t smem = 0;
+  // curved elements (atb_op_create_curved): per-node metrics and M J, per
+  // face node normals, face masses and neighbour nodes, the D matrix
+  bool curved = false;
+  double* d_D = nullptr;
+  double* d_G = nullptr;
+  double* d_MJn = nullptr;
+  double* d_fnrm = nullptr;
+  double* d_fMJ = nullptr;
+  int* d_fnb = nullptr;
   size_t stride() const { return (size_t)K * Np; }
 };
 
@@ -180,6 +190,7 @@ namespace {
 int cta_threads(int E, int Np) { return ((E * Np + 31) / 32) * 32; }
 
 size_t op_smem(const atb_op* op, int E, int pf = 0) {
+  if (op->curved) return curved_smem_bytes(op->vk, op->naux_used, op->Nq, E);
   return tend_smem_bytes(op->ns, op->npre, op->naux_used, op->dim, op->Nq, op->Np, op->Nfp, E, op->npv, false, pf);
 }
 
@@ -211,6 +222,12 @@ void fill_args(const atb_op* op, TendArgs& A) {
   A.lin_dirs = 0;
   A.naux_nl = op->naux_used;
   A.pf = 0;
+  A.Dmat = op->d_D;
+  A.G = op->d_G;
+  A.MJn = op->d_MJn;
+  A.fnrm = op->d_fnrm;
+  A.fMJ = op->d_fMJ;
+  A.fnb = op->d_fnb;
 }
 
 // EPI_ARK accumulators of one stage (see atb_tendency.cuh)
@@ -273,6 +290,7 @@ int reduce(atb_op* op, int kind, const double* const* p, const double* const* q,
     R.q[s] = q ? q[s < op->ns ? s : 0] : R.p[s];
   }
   R.partials = op->d_partials;
+  R.MJ = op->d_MJn;  // curved elements: per-node M J (null: weights x element Jacobian)
   {
     ProfScope ps(ATB_PROF_REDUCE, st);
     op->reducer(R, op->red_blocks, st);
@@ -311,6 +329,12 @@ extern "C" int atb_op_destroy(atb_op* op) {
   cudaFree(op->d_J);
   cudaFree(op->d_partials);
   cudaFree(op->d_red);
+  cudaFree(op->d_D);
+  cudaFree(op->d_G);
+  cudaFree(op->d_MJn);
+  cudaFree(op->d_fnrm);
+  cudaFree(op->d_fMJ);
+  cudaFree(op->d_fnb);
   if (op->h_red) cudaFreeHost(op->h_red);
   for (int i = 0; i < atb_op::kGeoRing; ++i) {
     if (op->geo_ev[i]) {
@@ -625,6 +649,93 @@ extern "C" int atb_op_set_aux(atb_op* op, const double* aux, void* stream) {
   // host or device source: unified addressing picks the direction
   CK(cudaMemcpyAsync(op->d_aux, aux, (size_t)op->naux * op->stride() * sizeof(double), cudaMemcpyDefault,
                      (cudaStream_t)stream));
+  return ATB_OK;
+}
+
+extern "C" int atb_op_create_curved(const atb_op_desc* d, const double* aux_host, const atb_curved_geometry* geo,
+                                    atb_op** out) {
+  if (!d || !geo || !out || !geo->metric || !geo->mj || !geo->normals || !geo->face_mj || !geo->nbr_node ||
+      !geo->btag)
+    return fail(ATB_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (d->dim != 3 || !d->stacked) return fail(ATB_ERR_INVALID, "curved elements: 3-D, stacked ordering");
+  if (d->law != LAW_EULER && d->law != LAW_EG && d->law != LAW_LEG)
+    return fail(ATB_ERR_INVALID, "curved elements: Euler, Euler-gravity or linear Euler-gravity");
+  if (d->precision != ATB_PREC_FP64) return fail(ATB_ERR_INVALID, "curved elements: FP64");
+  const int sf = d->surface_flux;
+  if (!(sf == ATB_FLUX_CENTRAL || sf == ATB_FLUX_RUSANOV ||
+        (d->law != LAW_LEG && (sf == ATB_FLUX_EC || sf == ATB_FLUX_KG))))
+    return fail(ATB_ERR_INVALID, "curved elements: surface flux central, Rusanov, entropy conservative or "
+                                 "Kennedy-Gruber");
+  if (d->bc_kind != ATB_BC_COPY && d->bc_kind != ATB_BC_REFLECT && d->bc_kind != ATB_BC_DIRICHLET)
+    return fail(ATB_ERR_INVALID, "curved elements: boundary state copy, reflect or Dirichlet");
+  atb_op* op = nullptr;
+  int rc = op_create_impl(d, 1, &aux_host, &op, d->naux > 0 && !aux_host);
+  if (rc) return rc;
+  tend_launch_fn fn = pick_launcher_curved(d->law, op->vk);
+  if (!fn) {
+    atb_op_destroy(op);
+    return fail(ATB_ERR_INVALID, "curved elements: no kernel for law %d, volume flux %d", d->law, d->volume_flux);
+  }
+  const int Nq = op->Nq, Np = op->Np, Nfp = op->Nfp, K = op->K;
+  const size_t KN = (size_t)K * Np, KF = (size_t)K * 6 * Nfp;
+  if (KN > (size_t)2147483647) {
+    atb_op_destroy(op);
+    return fail(ATB_ERR_INVALID, "curved elements: too many nodes");
+  }
+  // neighbour nodes -> int (-1 - tag on a boundary face), checked
+  std::vector<int> fnb(KF);
+  for (size_t i = 0; i < KF; ++i) {
+    const long long v = geo->nbr_node[i];
+    const int tag = geo->btag[i / ((size_t)6 * Nfp) * 6 + (i / Nfp) % 6];
+    if (v >= 0 && v < (long long)KN && tag == 0) {
+      fnb[i] = (int)v;
+    } else if (v < 0 && tag > 0) {
+      fnb[i] = -1 - tag;
+    } else {
+      atb_op_destroy(op);
+      return fail(ATB_ERR_INVALID, "curved elements: face node %zu has neighbour %lld with boundary tag %d", i, v,
+                  tag);
+    }
+  }
+  for (size_t i = 0; i < KN; ++i)
+    if (!(geo->mj[i] > 0)) {
+      atb_op_destroy(op);
+      return fail(ATB_ERR_INVALID, "curved elements: M J must be positive");
+    }
+  op->curved = true;
+  op->launch = fn;
+  // aux the kernels read: Phi (fluxes, wave speeds), grad Phi (weak-form
+  // gravity), the reference state (linear law; pde_level_balance)
+  int nu = 0;
+  if (d->law == LAW_EG) nu = d->pde_level_balance ? 6 : (op->vk == VK_WEAK ? 4 : 1);
+  if (d->law == LAW_LEG) nu = 6;
+  op->naux_used = std::min(nu, op->naux);
+  op->E = std::max(1, 128 / Np);
+  while (op->E > 1 && op_smem(op, op->E) > 100 * 1024) --op->E;
+  op->smem = op_smem(op, op->E);
+  if (op->smem > 227 * 1024 || cta_threads(op->E, Np) > 512) {
+    atb_op_destroy(op);
+    return fail(ATB_ERR_INVALID, "curved elements: element too large for one CTA");
+  }
+  if ((rc = dalloc(&op->d_D, (size_t)Nq * Nq)) || (rc = dalloc(&op->d_G, 9 * KN)) || (rc = dalloc(&op->d_MJn, KN)) ||
+      (rc = dalloc(&op->d_fnrm, 3 * KF)) || (rc = dalloc(&op->d_fMJ, KF)) || (rc = dalloc(&op->d_fnb, KF))) {
+    atb_op_destroy(op);
+    return rc;
+  }
+  cudaError_t e[6] = {
+      cudaMemcpy(op->d_D, op->D.data(), (size_t)Nq * Nq * sizeof(double), cudaMemcpyHostToDevice),
+      cudaMemcpy(op->d_G, geo->metric, 9 * KN * sizeof(double), cudaMemcpyHostToDevice),
+      cudaMemcpy(op->d_MJn, geo->mj, KN * sizeof(double), cudaMemcpyHostToDevice),
+      cudaMemcpy(op->d_fnrm, geo->normals, 3 * KF * sizeof(double), cudaMemcpyHostToDevice),
+      cudaMemcpy(op->d_fMJ, geo->face_mj, KF * sizeof(double), cudaMemcpyHostToDevice),
+      cudaMemcpy(op->d_fnb, fnb.data(), KF * sizeof(int), cudaMemcpyHostToDevice)};
+  for (int i = 0; i < 6; ++i)
+    if (e[i] != cudaSuccess) {
+      atb_op_destroy(op);
+      return fail(ATB_ERR_CUDA, "uploading the curved geometry failed");
+    }
+  *out = op;
   return ATB_OK;
 }
 
@@ -1663,6 +1774,7 @@ int fusion_check(atb_solver* s, cudaStream_t st) {
   if (R->law.kind != LAW_EG || L->law.kind != LAW_LEG || R->dim != 3 || L->vk != VK_WEAK) return ATB_OK;
   if (L->dirs != (1 << (R->dim - 1))) return ATB_OK;
   if (R->K != L->K || R->Np != L->Np || R->stacked != L->stacked) return ATB_OK;
+  if (R->curved || L->curved) return ATB_OK;  // the fused stage kernel has brick metrics
   const int na = R->dim + 3;
   if (R->naux < na || L->naux < na) return ATB_OK;
   tend_launch_fn f = pick_launcher_fused(R->dim, R->vk, R->Nq, R->sflux, L->sflux);

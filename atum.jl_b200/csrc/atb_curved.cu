@@ -1,0 +1,401 @@
+// DGSEM tendency on curved hexahedra (cubed-sphere shells): per-node metric
+// terms, per-face-node normals and face masses, neighbour traces through a
+// node-level face map.
+//
+// Restates, for one stage, src/dgsem.jl:217-306 (volumeterm!, weak form),
+// 470-561 (esvolumeterm_dir!, flux differencing: l_g = MJ g[dir, :] of both
+// nodes of every pair, all three rows of the two-point flux contracted with
+// them) and 683-732 (surfaceterm! with facenormal / faceMJ / faceix of a curved
+// grid), with the same epilogues as the brick kernels (atb_tendency.cuh).
+//
+// Mapping: one thread per LGL node, E elements per CTA.  The element's state
+// and aux, the per-node values the volume term reads of other nodes (weak
+// form: the contravariant flux rows MJ g[dir, :] . F; flux differencing: the
+// entropy-conservative / Kennedy-Gruber point values and MJ g) are staged in
+// shared memory.  Face tasks evaluate the numerical flux once per face node,
+// gather the neighbour trace from global memory and leave faceMJ * flux in a
+// shared slot; every node then subtracts the slots of its faces in face order.
+// Brick grids keep the specialised kernels (diagonal metrics, one flux row).
+#include "atb_curved.cuh"
+
+namespace atb {
+
+namespace {
+
+constexpr int CNS = 5;  // 3-D Euler / Euler-gravity / linear Euler-gravity states
+
+// physical flux rows F[d][s], d = 0..2 (src/balancelaws/*.jl flux)
+template <int LAW>
+__device__ __forceinline__ void flux_rows(const LawP& L, const double* q, const double* aux, double (*F)[CNS]) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) flux_dir<LAW, 3>(L, d, q, aux, F[d]);
+}
+
+// wavespeed(law, n, q, aux) for a general unit normal n
+template <int LAW>
+__device__ __forceinline__ double wavespeed_n(const LawP& L, const double* n, const double* q, const double* aux) {
+  if constexpr (LAW == LAW_LEG) {
+    return sqrt(L.gamma * aux[5] / aux[4]);  // sound speed of the reference state (aux: Phi, grad Phi, rho_ref, p_ref)
+  } else {
+    const double rho = q[0];
+    double u[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) u[c] = q[1 + c] / rho;
+    const double p = pressure_eg<3>(L.gamma, q, LAW == LAW_EG ? aux[0] : 0.0);
+    return fabs(dot<3>(n, u)) + sqrt(L.gamma * p / rho);
+  }
+}
+
+// two-point volume flux rows (entropy conservative / Kennedy-Gruber /
+// central) of the ordered pair (1 = own node, 2 = partner)
+template <int LAW, int VK>
+__device__ __forceinline__ void twopoint_rows(const LawP& L, const double* q1, const double* a1, const double* P1,
+                                              const double* q2, const double* a2, const double* P2,
+                                              double (*F)[CNS]) {
+  if constexpr (VK == VK_EC) {
+    const double Phi1 = (LAW == LAW_EG) ? a1[0] : 0.0, Phi2 = (LAW == LAW_EG) ? a2[0] : 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) ec_dir<LAW, 3>(L.gamma, d, q1[0], P1, Phi1, q2[0], P2, Phi2, F[d]);
+  } else if constexpr (VK == VK_KG) {
+    const double Phi1 = (LAW == LAW_EG) ? a1[0] : 0.0, Phi2 = (LAW == LAW_EG) ? a2[0] : 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) kg_dir<LAW, 3>(d, q1[0], P1, Phi1, q2[0], P2, Phi2, F[d]);
+  } else {
+    double G[3][CNS];
+    flux_rows<LAW>(L, q1, a1, F);
+    flux_rows<LAW>(L, q2, a2, G);
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+      for (int s = 0; s < CNS; ++s) F[d][s] = (F[d][s] + G[d][s]) / 2.0;
+  }
+}
+
+// boundarystate(law, problem, n, q-, aux-, tag) for a general normal
+__device__ __forceinline__ void boundary_state_n(const LawP& L, const double* n, int tag, const double* qm,
+                                                 double* qp) {
+  if (L.bc == BC_REFLECT) {
+    // rhou+ = rhou- - 2 (n . rhou-) n (experiment/euler_gravity/acousticwave.jl:17-22)
+    const double nm = dot<3>(n, qm + 1);
+    qp[0] = qm[0];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) qp[1 + k] = qm[1 + k] - 2.0 * nm * n[k];
+    qp[4] = qm[4];
+  } else if (L.bc == BC_DIRICHLET) {
+    const double* st = L.bc_state[tag == 1 ? 0 : 1];
+#pragma unroll
+    for (int s = 0; s < CNS; ++s) qp[s] = st[s];
+  } else {
+#pragma unroll
+    for (int s = 0; s < CNS; ++s) qp[s] = qm[s];
+  }
+}
+
+// numerical flux . n (src/numericalfluxes.jl:31-42 and the two-point fluxes
+// used as surface fluxes), general unit normal
+template <int LAW>
+__device__ __forceinline__ void surface_flux_n(const LawP& L, int kind, const double* n, const double* qm,
+                                               const double* am, const double* qp, const double* ap, double* nf) {
+  double F[3][CNS];
+  if (LAW != LAW_LEG && (kind == F_EC || kind == F_KG)) {
+    double Pm[NPreE<3>::v], Pp[NPreE<3>::v];
+    precompute_euler<3>(L.gamma, qm, LAW == LAW_EG ? am[0] : 0.0, Pm);
+    precompute_euler<3>(L.gamma, qp, LAW == LAW_EG ? ap[0] : 0.0, Pp);
+    if (kind == F_EC)
+      twopoint_rows<LAW, VK_EC>(L, qm, am, Pm, qp, ap, Pp, F);
+    else
+      twopoint_rows<LAW, VK_KG>(L, qm, am, Pm, qp, ap, Pp, F);
+  } else {
+    twopoint_rows<LAW, VK_CENTRAL>(L, qm, am, nullptr, qp, ap, nullptr, F);
+  }
+  double ws = 0.0;
+  if (kind == F_RUSANOV) ws = dmax(wavespeed_n<LAW>(L, n, qm, am), wavespeed_n<LAW>(L, n, qp, ap));
+#pragma unroll
+  for (int s = 0; s < CNS; ++s) {
+    double fn = F[0][s] * n[0];
+    fn = fn + F[1][s] * n[1];
+    fn = fn + F[2][s] * n[2];
+    nf[s] = (kind == F_RUSANOV) ? fn - ws * (qp[s] - qm[s]) / 2.0 : fn;
+  }
+}
+
+// per-node values staged for other nodes of the element: flux differencing
+// stages the two-point flux's point values (NPreE) and MJ g (9); the weak
+// form stages the contravariant flux rows (3 x NS)
+template <int VK> struct CurvedX {
+  static constexpr int v = (VK == VK_WEAK) ? 3 * CNS : NPreE<3>::v + 9;
+};
+
+template <int LAW, int VK>
+__global__ void __launch_bounds__(512) curved_kernel(const TendArgs A) {
+  constexpr int NS = CNS;
+  constexpr int NA = NAuxMax<LAW, 3>::v;
+  constexpr int NX = CurvedX<VK>::v;
+  extern __shared__ __align__(16) double smem[];
+  const int Nq = A.Nq, Np = A.Np, Nfp = A.Nfp, E = A.E, na = A.naux;
+  const int nqq = (Nq * Nq + 1) & ~1;
+  double* sD = smem;  // D[i][m] = l_m'(xi_i)
+  const size_t per = (size_t)(NS + na + NX) * Np + (size_t)6 * Nfp * NS;
+  const int tid = threadIdx.x;
+  const int el = tid / Np;
+  const int node = tid - el * Np;
+  const int e = blockIdx.x * E + el;
+  const bool active = el < E && e < A.K;
+  for (int i = tid; i < Nq * Nq; i += blockDim.x) sD[i] = A.Dmat[i];
+  double* base = smem + nqq + (size_t)(el < E ? el : 0) * per;
+  double* sq = base;
+  double* sa = sq + (size_t)NS * Np;
+  double* sx = sa + (size_t)na * Np;
+  const size_t stride = A.stride;
+  const size_t gid = (size_t)e * Np + node;
+  double qn[NS], an[NA];
+#pragma unroll
+  for (int k = 0; k < NA; ++k) an[k] = 0.0;
+  double MJ = 1.0, lg[3][3];
+  if (active) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      qn[s] = A.q[s][gid];
+      sq[s * Np + node] = qn[s];
+    }
+    for (int k = 0; k < na && k < NA; ++k) {
+      an[k] = A.aux[(size_t)k * stride + gid];
+      sa[k * Np + node] = an[k];
+    }
+    MJ = A.MJn[gid];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) lg[d][c] = A.G[((size_t)d * 3 + c) * stride + gid];
+    if constexpr (VK == VK_WEAK) {
+      double F[3][NS];
+      flux_rows<LAW>(A.law, qn, an, F);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        if (!((A.dirs >> d) & 1)) continue;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          double acc = 0.0;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) acc = acc + lg[d][c] * F[c][s];
+          sx[(d * NS + s) * Np + node] = acc * MJ;
+        }
+      }
+    } else {
+      double P[NPreE<3>::v];
+      precompute_euler<3>(A.law.gamma, qn, LAW == LAW_EG ? an[0] : 0.0, P);
+#pragma unroll
+      for (int k = 0; k < NPreE<3>::v; ++k) sx[k * Np + node] = P[k];
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          lg[d][c] = MJ * lg[d][c];
+          sx[(NPreE<3>::v + d * 3 + c) * Np + node] = lg[d][c];
+        }
+    }
+  }
+  __syncthreads();
+
+  // ---------------------------------------------------------- face tasks
+  const int ntask = E * 6 * Nfp;
+  for (int t = tid; t < ntask; t += blockDim.x) {
+    const int fe = t / (6 * Nfp);
+    const int r = t - fe * 6 * Nfp;
+    const int face = r / Nfp, j = r - face * Nfp;
+    const int k = face >> 1, side = face & 1;
+    const int eg = blockIdx.x * E + fe;
+    if (eg >= A.K || !((A.dirs >> k) & 1)) continue;
+    // face node j: tangential dimensions in increasing order, first fastest
+    const int t0 = j % Nq, t1 = j / Nq;
+    const int ek = side ? Nq - 1 : 0;
+    const int fn = (k == 0) ? ek + Nq * (t0 + Nq * t1) : (k == 1) ? t0 + Nq * (ek + Nq * t1) : t0 + Nq * (t1 + Nq * ek);
+    double* fb = smem + nqq + (size_t)fe * per;
+    const double* fq = fb;
+    const double* fa = fb + (size_t)NS * Np;
+    double* slot = fb + (size_t)(NS + na + NX) * Np;
+    const size_t fj = ((size_t)eg * 6 + face) * Nfp + j;
+    double n[3], qm[NS], am[NA], qp[NS], ap[NA];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) n[c] = A.fnrm[fj * 3 + c];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) qm[s] = fq[s * Np + fn];
+#pragma unroll
+    for (int c = 0; c < NA; ++c) am[c] = ap[c] = 0.0;
+    for (int c = 0; c < na && c < NA; ++c) am[c] = fa[c * Np + fn];
+    const int nb = A.fnb[fj];
+    if (nb >= 0) {
+#pragma unroll
+      for (int s = 0; s < NS; ++s) qp[s] = A.q[s][nb];
+      for (int c = 0; c < na && c < NA; ++c) ap[c] = A.aux[(size_t)c * stride + nb];
+    } else {
+      boundary_state_n(A.law, n, -1 - nb, qm, qp);
+#pragma unroll
+      for (int c = 0; c < NA; ++c) ap[c] = am[c];
+    }
+    double nf[NS];
+    surface_flux_n<LAW>(A.law, A.sflux, n, qm, am, qp, ap, nf);
+    const double fm = A.fMJ[fj];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) slot[(face * Nfp + j) * NS + s] = fm * nf[s];
+  }
+  __syncthreads();
+  if (!active) return;
+
+  // ------------------------------------------------------------- volume
+  const double MJI = 1.0 / MJ;
+  int ijk[3] = {node % Nq, (node / Nq) % Nq, node / (Nq * Nq)};
+  double T[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) T[s] = -0.0;
+  if ((A.dirs >> 2) & 1) add_sources<LAW, 3>(A.law, VK == VK_WEAK, qn, an, T);
+  for (int d = 0; d < 3; ++d) {
+    if (!((A.dirs >> d) & 1)) continue;
+    const int i = ijk[d];
+    const int step = (d == 0) ? 1 : (d == 1) ? Nq : Nq * Nq;
+    const int n0 = node - i * step;
+    if constexpr (VK == VK_WEAK) {
+      for (int m = 0; m < Nq; ++m) {
+        const double Dm = sD[m * Nq + i] * MJI;
+        const int nn = n0 + m * step;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) T[s] = T[s] + Dm * sx[(d * NS + s) * Np + nn];
+      }
+    } else {
+      double P1[NPreE<3>::v];
+#pragma unroll
+      for (int k = 0; k < NPreE<3>::v; ++k) P1[k] = sx[k * Np + node];
+      for (int m = 0; m < Nq; ++m) {
+        if (m == i) continue;  // -D_ii lg_i F + F lg_i D_ii: no contribution
+        const int nn = n0 + m * step;
+        double q2[NS], a2[NA], P2[NPreE<3>::v], lm[3];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) q2[s] = sq[s * Np + nn];
+#pragma unroll
+        for (int c = 0; c < NA; ++c) a2[c] = 0.0;
+        for (int c = 0; c < na && c < NA; ++c) a2[c] = sa[c * Np + nn];
+#pragma unroll
+        for (int k = 0; k < NPreE<3>::v; ++k) P2[k] = sx[k * Np + nn];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) lm[c] = sx[(NPreE<3>::v + d * 3 + c) * Np + nn];
+        double F[3][NS];
+        twopoint_rows<LAW, VK>(A.law, qn, an, P1, q2, a2, P2, F);
+        const double Ddn = MJI * sD[i * Nq + m], Dnd = MJI * sD[m * Nq + i];
+#pragma unroll
+        for (int s = 0; s < NS; ++s)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            T[s] = T[s] - Ddn * lg[d][c] * F[c][s];
+            T[s] = T[s] + F[c][s] * lm[c] * Dnd;
+          }
+      }
+    }
+  }
+  // ------------------------------------------------------------ surface
+  const double* slot = sx + (size_t)NX * Np;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    if (!((A.dirs >> k) & 1)) continue;
+    const int id = ijk[k];
+    if (id != 0 && id != Nq - 1) continue;
+    const int side = (id == Nq - 1) ? 1 : 0;
+    const int j = (k == 0) ? ijk[1] + Nq * ijk[2] : (k == 1) ? ijk[0] + Nq * ijk[2] : ijk[0] + Nq * ijk[1];
+    const int face = 2 * k + side;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) T[s] = T[s] - slot[(face * Nfp + j) * NS + s] * MJI;
+  }
+
+  // ----------------------------------------------------------- epilogue
+  switch (A.epi) {
+    case EPI_SET:
+#pragma unroll
+      for (int s = 0; s < NS; ++s) A.out[s][gid] = T[s];
+      break;
+    case EPI_ADD:
+#pragma unroll
+      for (int s = 0; s < NS; ++s) A.out[s][gid] = A.out[s][gid] + T[s];
+      break;
+    case EPI_LSRK: {
+      const double bdt = A.dte ? A.bdt * A.dte[e] : A.bdt;
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const double dqn = (A.a != 0.0) ? A.a * A.out[s][gid] + T[s] : T[s];
+        A.out[s][gid] = dqn;
+        A.out2[s][gid] = qn[s] + bdt * dqn;
+      }
+    } break;
+    case EPI_ARK:
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        // out holds N(Q), T = L(Q)
+        const double Ex = A.out[s][gid] - T[s];
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj)
+          if (A.acc[jj][0]) {
+            const double b0 = A.accin[jj][0] ? A.accin[jj][s][gid] : qn[s];
+            A.acc[jj][s][gid] = b0 + A.adt * (A.ca[jj] * Ex + A.cb[jj] * T[s]);
+          }
+      }
+      break;
+    case EPI_SUBOUT2:
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const double o2 = A.out2[s][gid];
+        A.out[s][gid] = T[s];
+        A.out2[s][gid] = o2 - T[s];
+      }
+      break;
+    case EPI_RLSRK:
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const double o2 = A.out2[s][gid];
+        A.out[s][gid] = T[s];
+        A.out2[s][gid] = A.a * o2 + T[s];
+      }
+      break;
+  }
+}
+
+template <int LAW, int VK>
+void curved_launch(const TendArgs& A, int grid, int block, size_t smem, cudaStream_t st) {
+  static size_t configured = 0;
+  if (smem > 48 * 1024 && smem > configured) {
+    if (cudaFuncSetAttribute(curved_kernel<LAW, VK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
+        cudaSuccess)
+      configured = smem;
+  }
+  curved_kernel<LAW, VK><<<grid, block, smem, st>>>(A);
+}
+
+}  // namespace
+
+size_t curved_smem_bytes(int vk, int naux, int Nq, int E) {
+  const int Np = Nq * Nq * Nq, Nfp = Nq * Nq;
+  const int nx = (vk == VK_WEAK) ? 3 * CNS : NPreE<3>::v + 9;
+  const size_t per = (size_t)(CNS + naux + nx) * Np + (size_t)6 * Nfp * CNS;
+  return sizeof(double) * ((size_t)((Nq * Nq + 1) & ~1) + per * E);
+}
+
+tend_launch_fn pick_launcher_curved(int law, int vk) {
+  switch (law) {
+    case LAW_EULER:
+      if (vk == VK_WEAK) return curved_launch<LAW_EULER, VK_WEAK>;
+      if (vk == VK_EC) return curved_launch<LAW_EULER, VK_EC>;
+      if (vk == VK_KG) return curved_launch<LAW_EULER, VK_KG>;
+      if (vk == VK_CENTRAL) return curved_launch<LAW_EULER, VK_CENTRAL>;
+      break;
+    case LAW_EG:
+      if (vk == VK_WEAK) return curved_launch<LAW_EG, VK_WEAK>;
+      if (vk == VK_EC) return curved_launch<LAW_EG, VK_EC>;
+      if (vk == VK_KG) return curved_launch<LAW_EG, VK_KG>;
+      if (vk == VK_CENTRAL) return curved_launch<LAW_EG, VK_CENTRAL>;
+      break;
+    case LAW_LEG:
+      if (vk == VK_WEAK) return curved_launch<LAW_LEG, VK_WEAK>;
+      if (vk == VK_CENTRAL) return curved_launch<LAW_LEG, VK_CENTRAL>;
+      break;
+  }
+  return nullptr;
+}
+
+}  // namespace atb

@@ -23,11 +23,13 @@ struct RedArgs {
   const double* p[5];  // state (first argument)
   const double* q[5];  // second argument (entropyproduct)
   double* partials;    // gridDim.x * 5
+  const double* MJ;    // per-node M J (curved elements), or null
 };
 
 constexpr int RED_THREADS = 256;
 
 __device__ __forceinline__ double node_mass(const RedArgs& R, int dim, size_t i) {
+  if (R.MJ) return R.MJ[i];
   const int e = (int)(i / R.Np), n = (int)(i - (size_t)e * R.Np), Nq = R.Nq;
   double w = R.w[n % Nq];
   if (dim > 1) w = w * R.w[(n / Nq) % Nq];

@@ -82,6 +82,16 @@ struct TendArgs {
   int naux_nl;  // aux components the explicit operator's faces read (fused launches stage more)
   int pf;       // epilogue input fields prefetched into shared memory (0: read at the end)
   size_t stride;      // K*Np
+  // curved elements (atb_curved.cu): D[i][m], metric terms G[(d*3 + c)*stride
+  // + gid] = d xi_d / d x_c, M J per node, per face node (e*6 + face)*Nfp + j
+  // the outward unit normal (3 values), faceMJ, and the neighbour's global
+  // node index (-1 - tag on a boundary face)
+  const double* Dmat;
+  const double* G;
+  const double* MJn;
+  const double* fnrm;
+  const double* fMJ;
+  const int* fnb;
   const double* q[5];
   double* out[5];
   double* out2[5];

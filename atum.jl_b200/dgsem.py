@@ -97,6 +97,8 @@ class DGSEM:
     def MJ(self) -> np.ndarray:
         """M * J per node, shape (K, Np) (src/dgsem.jl:43-45)."""
         c, g = self.grid.cell, self.grid
+        if hasattr(g, "geometry"):  # curved elements carry their own M J
+            return g.geometry()["MJ"]
         node = np.arange(c.Np)
         w = np.ones(c.Np)
         for d in range(g.dim):

@@ -11,6 +11,10 @@ library and the CPU oracle.
 * ``vortex_c1``   2-D Euler isentropic vortex, 8x8 elements, N=3, LSRK54
 * ``bubble_3d``   3-D Euler-gravity rising bubble, 16^3 elements, N=4, IMEX ARK23
 * ``sw_fplane``   rotating shallow water with bathymetry, 32^2 elements, N=4
+* ``sphere_acoustic_wave``  3-D Euler-gravity acoustic wave on a cubed-sphere
+  shell (experiment/euler_gravity/acousticwave.jl), N=5, KH=10, KV=5, IMEX ARK23
+* ``sphere_zonal_flow``     isothermal zonal flow on a small-planet shell
+  (experiment/euler_gravity/isothermal_zonal_flow.jl), N=3, KH=KV=5, IMEX ARK23
 """
 from __future__ import annotations
 
@@ -24,6 +28,7 @@ from .dgsem import DGSEM
 from .laws import (EulerLaw, EulerGravityLaw, LinearEulerGravityLaw, ShallowWaterLaw, ReflectiveWall, Coriolis,
                    RusanovFlux, EntropyConservativeFlux, KennedyGruberFlux, FluxDifferencingForm)
 from .cell import LobattoCell, brickgrid, min_node_distance
+from .cubedsphere import cubedspheregrid
 
 
 @dataclass
@@ -150,6 +155,105 @@ def bubble_3d(N=4, K=16, L=10e3, imex=True, steps=200, dt=None, precision="fp64"
                     adjust_final=False, extra={"steps": steps})
     dt = dt if dt is not None else 0.3 * dz / 340.0
     return Case("bubble_3d_lsrk", dg, q0, dt, steps * dt, extra={"steps": steps})
+
+
+# ------------------------------------------------ cubed-sphere shells
+_EARTH_RADIUS = 6.371229e6
+
+
+def _isothermal_reference(a):
+    """Isothermal (T_ref = 300 K) hydrostatic reference state above radius a
+    (acousticwave.jl:25-41, isothermal_zonal_flow.jl:42-61)."""
+    def ref(law, x):
+        r = np.sqrt(np.sum(x * x, axis=0))
+        z = r - a
+        cv_d = 719.0
+        R_d = law.gamma * cv_d - cv_d
+        T_ref = 300.0
+        delta = law.grav / (R_d * T_ref)
+        rho_s = 1e5 / (T_ref * R_d)
+        rho = rho_s * np.exp(-delta * z)
+        return rho, rho * R_d * T_ref
+    return ref
+
+
+def _sphere_case(name, law, grid, q0, dt, steps, imex, vflux):
+    vf = FluxDifferencingForm(EntropyConservativeFlux() if vflux == "ec" else KennedyGruberFlux())
+    dg = DGSEM(law=law, grid=grid, volume_form=vf, surface_numericalflux=RusanovFlux())
+    if imex:
+        lindg = DGSEM(law=LinearEulerGravityLaw(law), grid=grid, surface_numericalflux=RusanovFlux(),
+                      auxstate=dg.auxstate_host(), directions=(3,))
+        return Case(name, dg, q0(dg), dt, steps * dt, solver="ARK23", lindg=lindg, split_rhs=False,
+                    adjust_final=False, extra={"steps": steps})
+    return Case(name, dg, q0(dg), dt, steps * dt, adjust_final=False, extra={"steps": steps})
+
+
+def sphere_acoustic_wave(N=5, KH=10, KV=5, steps=10, imex=True, dt=None, vflux="ec"):
+    """Acoustic wave on an Earth-radius shell 10 km deep (cubed sphere, KH x KH
+    elements per panel, KV layers, order N): isothermal atmosphere at rest
+    with a pressure perturbation of 100 Pa x (1 + cos(pi beta))/2 x sin(pi z/H)
+    around (lon, lat) = (0, 0), beta = min(1, 3 * great-circle angle);
+    reflective inner and outer spheres; EC volume flux, Rusanov surface flux,
+    IMEX ARK23 (split_rhs = false) with dt = 100 (H/KV) / 330 / N^2
+    (acousticwave.jl:43-111)."""
+    a, H = _EARTH_RADIUS, 10e3
+    law = EulerGravityLaw(3, sphere=True, problem=ReflectiveWall(referencestate=_isothermal_reference(a)))
+    cell = LobattoCell(N + 1, N + 1, N + 1)
+    grid = cubedspheregrid(cell, _vec(a, a + H, KV), KH)
+
+    def q0(dg):
+        x = grid.points()
+        aux = dg.auxstate_host()
+        Phi, p_ref = aux[0], aux[5]
+        cv_d = 719.0
+        R_d = law.gamma * cv_d - cv_d
+        r = np.sqrt(np.sum(x * x, axis=0))
+        z = r - a
+        lon = np.arctan2(x[1], x[0])
+        lat = np.arcsin(x[2] / r)
+        beta = np.minimum(1.0, 3.0 * np.arccos(np.cos(lat) * np.cos(lon)))
+        p = p_ref + 100.0 * (1 + np.cos(np.pi * beta)) / 2 * np.sin(np.pi * z / H)
+        rho = p / (R_d * 300.0)
+        zero = np.zeros_like(rho)
+        return _pack(rho, zero, zero, zero, rho * (cv_d * 300.0 + Phi))
+
+    dt = dt if dt is not None else 100 * (H / KV) / 330.0 / N ** 2
+    return _sphere_case("sphere_acoustic_wave", law, grid, q0, dt, steps, imex, vflux)
+
+
+def sphere_zonal_flow(N=3, KH=5, KV=5, steps=10, imex=True, dt=None, vflux="ec"):
+    """Isothermal zonal flow on a small planet (radius 6.371229e6 / 125, model
+    top 10 km): u = 20 (1 + z/a) cos(lat) m/s eastward in the balanced
+    isothermal (300 K) state; reflective inner and outer spheres; EC volume
+    flux, Rusanov surface flux, IMEX ARK23 (split_rhs = false) with
+    dt = 3 dz / 330, dz the smallest radial node distance
+    (isothermal_zonal_flow.jl:63-125)."""
+    a, top = _EARTH_RADIUS / 125, 10e3
+    law = EulerGravityLaw(3, sphere=True, problem=ReflectiveWall(referencestate=_isothermal_reference(a)))
+    cell = LobattoCell(N + 1, N + 1, N + 1)
+    grid = cubedspheregrid(cell, _vec(a, a + top, KV), KH)
+
+    def q0(dg):
+        x = grid.points()
+        Phi = dg.auxstate_host()[0]
+        cv_d = 719.0
+        R_d = law.gamma * cv_d - cv_d
+        r = np.sqrt(np.sum(x * x, axis=0))
+        z = r - a
+        lon = np.arctan2(x[1], x[0])
+        lat = np.arcsin(x[2] / r)
+        u0, T0, g = 20.0, 300.0, law.grav
+        us = u0 * (1 + z / a) * np.cos(lat)  # zonal wind; meridional and radial zero
+        u = [-np.sin(lon) * us, np.cos(lon) * us, np.zeros_like(us)]
+        f2 = z / a + z ** 2 / (2 * a ** 2)
+        prefac = u0 ** 2 / (R_d * T0)
+        p = 1e5 * np.exp(prefac * f2 * np.cos(lat) ** 2 - prefac * np.sin(lat) ** 2 / 2 - g * z / (R_d * T0))
+        rho = p / (R_d * T0)
+        ke = (u[0] ** 2 + u[1] ** 2 + u[2] ** 2) / 2
+        return _pack(rho, rho * u[0], rho * u[1], rho * u[2], rho * (cv_d * T0 + ke + Phi))
+
+    dt = dt if dt is not None else 3 * min_node_distance(grid, dims=(3,)) / 330.0
+    return _sphere_case("sphere_zonal_flow", law, grid, q0, dt, steps, imex, vflux)
 
 
 # ------------------------------------------------------ shallow water, C3

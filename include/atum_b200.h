@@ -121,6 +121,38 @@ int atb_op_set_aux(atb_op* op, const double* aux, void* stream);
 int atb_op_destroy(atb_op* op);
 int atb_op_dims(const atb_op* op, int* ns, int* K, int* Np);
 
+/* Curved elements: DGSEM(; law, grid = cubedspheregrid(cell, vr, KH), ...)
+ * (src/dgsem.jl:38-56 with Bennu's metrics(grid) / facemetrics(grid) of a
+ * curved grid; experiment/euler_gravity/acousticwave.jl:90-99).  The
+ * descriptor gives law, order, forms, fluxes, directions, constants and the
+ * element counts K = {6*KH, KH, KV} with stacked = 1 (vertex vectors: any
+ * increasing vectors of K[d]+1 values; they are not read for the geometry).
+ * Host arrays, Np = Nq^3, Nfp = Nq^2, face f = 2*dir + side, face node j
+ * enumerating the two tangential dimensions in increasing order, the lower
+ * one fastest:
+ *   metric[((dir*3 + c)*K + e)*Np + n]  d xi_dir / d x_c
+ *   mj[e*Np + n]                        M J (LGL weights times the Jacobian)
+ *   normals[((e*6 + f)*Nfp + j)*3 + c]  outward unit normal
+ *   face_mj[(e*6 + f)*Nfp + j]          face weights times |J grad xi_dir|
+ *   nbr_node[(e*6 + f)*Nfp + j]         the neighbour's node e'*Np + n', or
+ *                                       -1 on a boundary face
+ *   btag[e*6 + f]                       boundary tag (0 interior)
+ * 3-D Euler, Euler-gravity (weak form; flux differencing with the central,
+ * entropy-conservative or Kennedy-Gruber flux) and linear Euler-gravity (weak
+ * form); surface fluxes central, Rusanov, entropy conservative,
+ * Kennedy-Gruber; FP64.  The operator works with every solver, ARK23's banded
+ * vertical solve included (one band per vertical line of nodes). */
+typedef struct {
+  const double* metric;
+  const double* mj;
+  const double* normals;
+  const double* face_mj;
+  const long long* nbr_node;
+  const int* btag;
+} atb_curved_geometry;
+int atb_op_create_curved(const atb_op_desc* desc, const double* aux_host, const atb_curved_geometry* geo,
+                         atb_op** out);
+
 /* Multi-instance batching (no reference counterpart; the reference builds one
  * DGSEM per problem, src/dgsem.jl:38-56, and steps each alone).  n instances
  * that share law, order, forms, fluxes, directions, precision, constants and

@@ -136,6 +136,13 @@ struct Op {
   std::vector<double> face_w;   // 6 x Nfp face weight
   std::vector<double> points;   // dim x K x Np
   std::vector<double> v[3];
+  // curved elements (orc_op_set_curved): per-node metric terms
+  // G[((dir*3 + c)*K + e)*Np + n] = d xi_dir / d x_c, per-face-node outward
+  // unit normals fn[((e*6 + f)*Nfp + j)*3 + c], face mass faceMJ[(e*6 + f)*Nfp + j]
+  // and the neighbour's global node index fnb (-1 on a boundary face)
+  bool curved = false;
+  std::vector<double> G, fn, fMJ;
+  std::vector<long long> fnb;
 
   int elem_of(const int* idx) const {
     if (stacked) {
@@ -161,6 +168,10 @@ struct Op {
     ijk[2] = n / (Nq * Nq);
   }
   double g(int e, int dir, int d) const { return dir == d ? 2.0 / h[e * 3 + d] : 0.0; }
+  // metric term of node id = e*Np + n (src/dgsem.jl:38-56 metrics(grid))
+  double gn(size_t id, int dir, int d) const {
+    return curved ? G[((size_t)dir * 3 + d) * (size_t)K * Np + id] : g((int)(id / Np), dir, d);
+  }
 };
 
 void op_build(Op& o, const orc_desc* d, const double* aux) {
@@ -318,7 +329,7 @@ void volume_weak(const Op& o, double* dq, const double* q, bool increment) {
         for (int dd = 0; dd < o.ndirs; ++dd) {
           int dir = o.dirs[dd];
           double acc = 0;
-          for (int c = 0; c < dim; ++c) acc = acc + o.g(e, dir, c) * F[c][s];
+          for (int c = 0; c < dim; ++c) acc = acc + o.gn(id, dir, c) * F[c][s];
           lF[((size_t)n * 3 + dd) * 5 + s] = acc * MJ;
         }
     }
@@ -374,7 +385,7 @@ void volume_fd_dir(const Op& o, int dir, double* dq, const double* q, bool incre
       }
       double MJI = o.MJI[id];
       double lg_i[3];
-      for (int c = 0; c < dim; ++c) lg_i[c] = o.MJ[id] * o.g(e, dir, c);
+      for (int c = 0; c < dim; ++c) lg_i[c] = o.MJ[id] * o.gn(id, dir, c);
       const int id_ = ijk[dir];
       for (int pass = 0; pass < (symmetric ? 2 : 1); ++pass) {
         double* acc = pass ? d2 : d1;
@@ -388,7 +399,7 @@ void volume_fd_dir(const Op& o, int dir, double* dq, const double* q, bool incre
           gather(o.aux.data(), A, st, ild, a2);
           twopointflux(o.volume_flux, L, q1, a1, q2, a2, F);
           double lg_n[3];
-          for (int c = 0; c < dim; ++c) lg_n[c] = o.MJ[ild] * o.g(e, dir, c);
+          for (int c = 0; c < dim; ++c) lg_n[c] = o.MJ[ild] * o.gn(ild, dir, c);
           for (int s = 0; s < S; ++s) {
             double Ddn = MJI * o.D[id_ * Nq + m];
             double Dnd = MJI * o.D[m * Nq + id_];
@@ -447,7 +458,7 @@ void volume_fd_naive(const Op& o, double* dq, const double* q, bool increment) {
             double Din = MJI * o.D[ii * Nq + m];
             double Dni = MJI * o.D[m * Nq + ii];
             for (int c = 0; c < dim; ++c) {
-              double lgi = o.MJ[id] * o.g(e, dir, c), lgn = o.MJ[ild] * o.g(e, dir, c);
+              double lgi = o.MJ[id] * o.gn(id, dir, c), lgn = o.MJ[ild] * o.gn(ild, dir, c);
               dqn[s] = dqn[s] - Din * lgi * F[c][s];
               dqn[s] = dqn[s] + F[c][s] * lgn * Dni;
             }
@@ -464,6 +475,39 @@ void surface(const Op& o, double* dq, const double* q) {
   const Law& L = o.law;
   const int Nq = o.Nq, Np = o.Np, S = L.ns, A = L.naux, dim = o.dim;
   const size_t st = (size_t)o.K * Np;
+  if (o.curved) {
+    // surfaceterm! (src/dgsem.jl:683-732) with facenormal / faceMJ / faceix
+    // of a curved grid: per-face-node normal and face mass, neighbour node
+    // from the face map
+    par_for(o.K, [&](int e) {
+      for (int dd = 0; dd < o.ndirs; ++dd) {
+        const int k = o.dirs[dd];
+        for (int f = 0; f < 2; ++f) {
+          const int face = 2 * k + f;
+          const int tag = o.btag[e * 6 + face];
+          for (int j = 0; j < o.Nfp; ++j) {
+            const size_t fj = ((size_t)e * 6 + face) * o.Nfp + j;
+            const int nm = o.face_node[face * o.Nfp + j];
+            const size_t idm = (size_t)e * Np + nm;
+            const double* nvec = &o.fn[fj * 3];
+            double qm[5], am[8], qp[5], ap[8], nf[5];
+            gather(o.aux.data(), A, st, idm, am);
+            gather(q, S, st, idm, qm);
+            if (tag == 0) {
+              const size_t idp = (size_t)o.fnb[fj];
+              gather(q, S, st, idp, qp);
+              gather(o.aux.data(), A, st, idp, ap);
+            } else {
+              boundarystate(L, nvec, qm, am, tag, qp, ap);
+            }
+            surfaceflux(o.surface_flux, L, nvec, qm, am, qp, ap, nf);
+            for (int s = 0; s < S; ++s) dq[s * st + idm] = dq[s * st + idm] - o.fMJ[fj] * nf[s] * o.MJI[idm];
+          }
+        }
+      }
+    });
+    return;
+  }
   par_for(o.K, [&](int e) {
     for (int dd = 0; dd < o.ndirs; ++dd) {
       int k = o.dirs[dd];
@@ -876,6 +920,25 @@ void* orc_op_create(const orc_desc* d, const double* aux) {
 void orc_op_destroy(void* op) { delete (Op*)op; }
 void orc_op_apply(void* op, double* dq, const double* q, double t, int increment) {
   op_apply(*(Op*)op, dq, q, t, increment != 0);
+}
+int orc_op_set_curved(void* op, const double* metric, const double* mj, const double* normals,
+                      const double* face_mj, const long long* nbr_node, const int* btag, const double* points) {
+  Op& o = *(Op*)op;
+  if (o.dim != 3 || !metric || !mj || !normals || !face_mj || !nbr_node || !btag) return -1;
+  const size_t KN = (size_t)o.K * o.Np, KF = (size_t)o.K * 6 * o.Nfp;
+  o.curved = true;
+  o.G.assign(metric, metric + 9 * KN);
+  o.MJ.assign(mj, mj + KN);
+  for (size_t i = 0; i < KN; ++i) o.MJI[i] = 1.0 / o.MJ[i];
+  o.fn.assign(normals, normals + 3 * KF);
+  o.fMJ.assign(face_mj, face_mj + KF);
+  o.fnb.assign(nbr_node, nbr_node + KF);
+  o.btag.assign(btag, btag + (size_t)o.K * 6);
+  for (size_t i = 0; i < KF; ++i)
+    if (o.fnb[i] >= (long long)KN || (o.fnb[i] < 0 && o.btag[i / (6 * o.Nfp) * 6 + (i / o.Nfp) % 6] == 0))
+      return -1;
+  if (points) o.points.assign(points, points + 3 * KN);
+  return 0;
 }
 void orc_points(void* op, double* x) {
   Op* o = (Op*)op;

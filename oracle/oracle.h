@@ -44,6 +44,15 @@ typedef struct {
 void* orc_op_create(const orc_desc* d, const double* aux);
 void orc_op_destroy(void* op);
 void orc_op_apply(void* op, double* dq, const double* q, double t, int increment);
+/* curved 3-D elements (a cubed-sphere shell): per-node metric terms
+ * metric[((dir*3 + c)*K + e)*Np + n] = d xi_dir / d x_c, M J per node, per face
+ * node (face f = 2*dir + side, face node j as the brick's face tables) the
+ * outward unit normal normals[((e*6 + f)*Nfp + j)*3 + c], faceMJ, and the
+ * neighbour's global node index e'*Np + n' (-1 with btag[e*6 + f] != 0 on a
+ * boundary face); points (3 x K x Np) may be NULL.  Returns 0, or -1 on bad
+ * input.  Replaces the brick geometry the descriptor built. */
+int orc_op_set_curved(void* op, const double* metric, const double* mj, const double* normals,
+                      const double* face_mj, const long long* nbr_node, const int* btag, const double* points);
 void orc_points(void* op, double* x);   /* dim x K x Np */
 void orc_mj(void* op, double* mj);      /* K x Np */
 

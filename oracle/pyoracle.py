@@ -53,6 +53,8 @@ def lib():
         L.orc_op_create.argtypes = [C.POINTER(_Desc), dp]
         L.orc_op_destroy.argtypes = [vp]
         L.orc_op_apply.argtypes = [vp, dp, dp, C.c_double, C.c_int]
+        L.orc_op_set_curved.restype = C.c_int
+        L.orc_op_set_curved.argtypes = [vp, dp, dp, dp, dp, C.POINTER(C.c_longlong), C.POINTER(C.c_int), dp]
         L.orc_points.argtypes = [vp, dp]
         L.orc_mj.argtypes = [vp, dp]
         L.orc_solver_create.restype = vp
@@ -123,6 +125,18 @@ class DGSEM:
         self.Np = dg.grid.cell.Np
         self.dim = dg.grid.dim
         self.h = lib().orc_op_create(C.byref(self._desc), _dp(aux) if aux.size else None)
+        geo = getattr(dg.grid, "geometry", None)
+        if geo is not None:
+            G = geo()
+            arrs = [np.ascontiguousarray(G[k], dtype=np.float64) for k in ("g", "MJ", "normals", "faceMJ", "x")]
+            nb = np.ascontiguousarray(G["nbr_node"], dtype=np.int64)
+            bt = np.ascontiguousarray(G["btag"], dtype=np.int32)
+            self._geo = (arrs, nb, bt)
+            rc = lib().orc_op_set_curved(self.h, _dp(arrs[0]), _dp(arrs[1]), _dp(arrs[2]), _dp(arrs[3]),
+                                         nb.ctypes.data_as(C.POINTER(C.c_longlong)),
+                                         bt.ctypes.data_as(C.POINTER(C.c_int)), _dp(arrs[4]))
+            if rc != 0:
+                raise ValueError("curved geometry rejected by the oracle")
 
     def __del__(self):
         if getattr(self, "h", None) and _LIB is not None:
