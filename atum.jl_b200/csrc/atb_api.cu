@@ -664,9 +664,8 @@ extern "C" int atb_op_create_curved(const atb_op_desc* d, const double* aux_host
   if (d->precision != ATB_PREC_FP64) return fail(ATB_ERR_INVALID, "curved elements: FP64");
   const int sf = d->surface_flux;
   if (!(sf == ATB_FLUX_CENTRAL || sf == ATB_FLUX_RUSANOV ||
-        (d->law != LAW_LEG && (sf == ATB_FLUX_EC || sf == ATB_FLUX_KG))))
-    return fail(ATB_ERR_INVALID, "curved elements: surface flux central, Rusanov, entropy conservative or "
-                                 "Kennedy-Gruber");
+        (d->law != LAW_LEG && sf >= ATB_FLUX_EC && sf <= ATB_FLUX_MATRIX)))
+    return fail(ATB_ERR_INVALID, "curved elements: no surface flux %d for law %d", sf, d->law);
   if (d->bc_kind != ATB_BC_COPY && d->bc_kind != ATB_BC_REFLECT && d->bc_kind != ATB_BC_DIRICHLET)
     return fail(ATB_ERR_INVALID, "curved elements: boundary state copy, reflect or Dirichlet");
   atb_op* op = nullptr;

@@ -91,11 +91,141 @@ __device__ __forceinline__ void boundary_state_n(const LawP& L, const double* n,
   }
 }
 
+// Roe flux for a general unit normal (src/balancelaws/euler.jl:91-138,
+// euler_gravity.jl:149-198): the average of the two sides' normal fluxes minus
+// the Roe-averaged characteristic dissipation
+template <int LAW>
+__device__ __forceinline__ void roe_n(const LawP& L, const double* n, const double* qm, const double* am,
+                                      const double* qp, const double* ap, double* nf) {
+  const double g = L.gamma;
+  const double Phi = (LAW == LAW_EG) ? am[0] : 0.0;
+  double Fm[3][CNS], Fp[3][CNS];
+  flux_rows<LAW>(L, qm, am, Fm);
+  flux_rows<LAW>(L, qp, ap, Fp);
+  const double rm = qm[0], rp = qp[0];
+  double um[3], up[3], u[3], du[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) { um[c] = qm[1 + c] / rm; up[c] = qp[1 + c] / rp; }
+  const double pm = pressure_eg<3>(g, qm, Phi), pp = pressure_eg<3>(g, qp, Phi);
+  const double hm = qm[4] / rm + pm / rm, hp = qp[4] / rp + pp / rp;
+  const double cm = sqrt(g * pm / rm), cp = sqrt(g * pp / rp);
+  const double srm = sqrt(rm), srp = sqrt(rp);
+  const double rho = sqrt(rm * rp);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) { u[c] = roe_avg(srm, srp, um[c], up[c]); du[c] = up[c] - um[c]; }
+  const double h = roe_avg(srm, srp, hm, hp);
+  const double c = roe_avg(srm, srp, cm, cp);
+  const double un = dot<3>(u, n);
+  const double drho = rp - rm, dp = pp - pm;
+  const double dun = dot<3>(du, n);
+  const double cm2 = 1.0 / (c * c);
+  const double w1 = fabs(un - c) * (dp - rho * c * dun) * cm2 / 2.0;
+  const double w2 = fabs(un + c) * (dp + rho * c * dun) * cm2 / 2.0;
+  const double w3 = fabs(un) * (drho - dp * cm2);
+  const double w4 = fabs(un) * rho;
+  double fpv[CNS];
+  fpv[0] = (w1 + w2 + w3) / 2.0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+    fpv[1 + k] = (w1 * (u[k] - c * n[k]) + w2 * (u[k] + c * n[k]) + w3 * u[k] + w4 * (du[k] - dun * n[k])) / 2.0;
+  const double ke = (LAW == LAW_EG) ? w3 * (dot<3>(u, u) / 2.0 + Phi) : w3 * dot<3>(u, u) / 2.0;
+  fpv[4] = (w1 * (h - c * un) + w2 * (h + c * un) + ke + w4 * (dot<3>(u, du) - un * dun)) / 2.0;
+#pragma unroll
+  for (int s = 0; s < CNS; ++s) {
+    double fn = (Fm[0][s] + Fp[0][s]) * n[0];
+    fn = fn + (Fm[1][s] + Fp[1][s]) * n[1];
+    fn = fn + (Fm[2][s] + Fp[2][s]) * n[2];
+    nf[s] = fn / 2.0 - fpv[s];
+  }
+}
+
+// matrix-dissipation flux for a general unit normal (src/balancelaws/euler.jl:
+// 198-256, euler_gravity.jl:271-332): the entropy-conservative flux . n minus
+// half the entropy-variable jump scaled by the eigen-decomposition of the
+// averaged state
+template <int LAW>
+__device__ __forceinline__ void matrix_n(const LawP& L, const double* n, const double* qm, const double* am,
+                                         const double* qp, const double* ap, double* nf) {
+  const double g = L.gamma;
+  const double Phim = (LAW == LAW_EG) ? am[0] : 0.0, Phip = (LAW == LAW_EG) ? ap[0] : 0.0;
+  double Pm[NPreE<3>::v], Pp[NPreE<3>::v];
+  precompute_euler<3>(g, qm, Phim, Pm);
+  precompute_euler<3>(g, qp, Phip, Pp);
+  double ec[CNS];
+  {
+    double F[3][CNS];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) ec_dir<LAW, 3>(g, d, qm[0], Pm, Phim, qp[0], Pp, Phip, F[d]);
+#pragma unroll
+    for (int s = 0; s < CNS; ++s) {
+      double fn = F[0][s] * n[0];
+      fn = fn + F[1][s] * n[1];
+      ec[s] = fn + F[2][s] * n[2];
+    }
+  }
+  const double rm = qm[0], rp = qp[0];
+  const double bm = Pm[4], bp = Pp[4];
+  const double Phi_avg = (Phim + Phip) / 2.0;
+  const double rho_log = logavg(rm, rp);
+  const double b_log = logavg(bm, bp);
+  double ua[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) ua[c] = (Pm[c] + Pp[c]) / 2.0;
+  const double p_avg = ((rm + rp) / 2.0) / (2.0 * ((bm + bp) / 2.0));
+  // the norms of the velocities (not their squares), as the reference has it
+  const double u2_bar = 2.0 * sqrt(dot<3>(ua, ua)) - (sqrt(Pm[5]) + sqrt(Pp[5])) / 2.0;
+  double h_bar = g / (2.0 * b_log * (g - 1.0)) + u2_bar / 2.0;
+  if (LAW == LAW_EG) h_bar = h_bar + Phi_avg;
+  const double c_bar = sqrt(g * p_avg / rho_log);
+  double umc[3], upc[3], ut[3];
+  const double un = dot<3>(ua, n);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    umc[k] = ua[k] - c_bar * n[k];
+    upc[k] = ua[k] + c_bar * n[k];
+    ut[k] = ua[k] - un * n[k];
+  }
+  double vm[CNS], vp[CNS], dv[CNS];
+  entropyvars<LAW, 3>(L, qm, am, vm);
+  entropyvars<LAW, 3>(L, qp, ap, vp);
+#pragma unroll
+  for (int s = 0; s < CNS; ++s) dv[s] = vp[s] - vm[s];
+  const double l1 = fabs(un - c_bar) * rho_log / (2.0 * g);
+  const double l2 = fabs(un) * rho_log * (g - 1.0) / g;
+  const double l3 = fabs(un + c_bar) * rho_log / (2.0 * g);
+  const double l4 = fabs(un) * p_avg;
+  double k2 = u2_bar / 2.0;
+  if (LAW == LAW_EG) k2 = k2 + Phi_avg;
+  const double w1 = l1 * (dv[0] + dot<3>(umc, dv + 1) + (h_bar - c_bar * un) * dv[4]);
+  const double w2 = l2 * (dv[0] + dot<3>(ua, dv + 1) + k2 * dv[4]);
+  const double w3 = l3 * (dv[0] + dot<3>(upc, dv + 1) + (h_bar + c_bar * un) * dv[4]);
+  const double ndv = dot<3>(n, dv + 1);
+  double Dm[CNS];
+  Dm[0] = w1 + w2 + w3;
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+    Dm[1 + k] = w1 * umc[k] + w2 * ua[k] + w3 * upc[k] + l4 * (dv[1 + k] - ndv * n[k] + dv[4] * ut[k]);
+  Dm[4] = w1 * (h_bar - c_bar * un) + w2 * k2 + w3 * (h_bar + c_bar * un) +
+          l4 * (dot<3>(ut, dv + 1) + dv[4] * (dot<3>(ua, ua) - un * un));
+#pragma unroll
+  for (int s = 0; s < CNS; ++s) nf[s] = ec[s] - Dm[s] / 2.0;
+}
+
 // numerical flux . n (src/numericalfluxes.jl:31-42 and the two-point fluxes
 // used as surface fluxes), general unit normal
 template <int LAW>
 __device__ __forceinline__ void surface_flux_n(const LawP& L, int kind, const double* n, const double* qm,
                                                const double* am, const double* qp, const double* ap, double* nf) {
+  if constexpr (LAW != LAW_LEG) {
+    if (kind == F_ROE) {
+      roe_n<LAW>(L, n, qm, am, qp, ap, nf);
+      return;
+    }
+    if (kind == F_MATRIX) {
+      matrix_n<LAW>(L, n, qm, am, qp, ap, nf);
+      return;
+    }
+  }
   double F[3][CNS];
   if (LAW != LAW_LEG && (kind == F_EC || kind == F_KG)) {
     double Pm[NPreE<3>::v], Pp[NPreE<3>::v];

@@ -139,9 +139,10 @@ int atb_op_dims(const atb_op* op, int* ns, int* K, int* Np);
  *   btag[e*6 + f]                       boundary tag (0 interior)
  * 3-D Euler, Euler-gravity (weak form; flux differencing with the central,
  * entropy-conservative or Kennedy-Gruber flux) and linear Euler-gravity (weak
- * form); surface fluxes central, Rusanov, entropy conservative,
- * Kennedy-Gruber; FP64.  The operator works with every solver, ARK23's banded
- * vertical solve included (one band per vertical line of nodes). */
+ * form); surface fluxes central and Rusanov, and for the nonlinear laws also
+ * entropy conservative, Kennedy-Gruber, Roe and matrix dissipation; FP64.
+ * The operator works with every solver, ARK23's banded vertical solve
+ * included (one band per vertical line of nodes). */
 typedef struct {
   const double* metric;
   const double* mj;
