@@ -194,19 +194,20 @@ def _build_geometry(g: CubedSphereGrid) -> dict:
         fMJ[:, f] = fw[None, :] * mag
     xf = x.reshape(3, K, Np)
     # neighbours: faces matched by their centres, then nodes by coordinates
+    fn_all = np.stack([fn.reshape(-1) for fn in fnodes])          # (6, Nfp)
+    fx = xf[:, :, fn_all]                                           # (3, K, 6, Nfp)
     scale = float(g.vr[-1])
-    key = lambda p: tuple(np.round(p / scale * 1e9).astype(np.int64))  # noqa: E731
+    keys = np.round(fx.mean(axis=3) / scale * 1e9).astype(np.int64)  # (3, K, 6)
     centre = {}
     for e in range(K):
         for f in range(6):
-            nf = fnodes[f].reshape(-1)
-            centre.setdefault(key(xf[:, e, nf].mean(axis=1)), []).append((e, f))
+            centre.setdefault((keys[0, e, f], keys[1, e, f], keys[2, e, f]), []).append((e, f))
     nbr_node = np.full((K, 6, Nfp), -1, dtype=np.int64)
+    partner = np.full((K, 6, Nfp), -1, dtype=np.int64)  # (e2*6 + f2)*Nfp + j2 of the matching face node
     btag = np.zeros((K, 6), dtype=np.int32)
     for e in range(K):
         for f in range(6):
-            nf = fnodes[f].reshape(-1)
-            cands = [(e2, f2) for (e2, f2) in centre[key(xf[:, e, nf].mean(axis=1))] if e2 != e]
+            cands = [c for c in centre[(keys[0, e, f], keys[1, e, f], keys[2, e, f])] if c[0] != e]
             if not cands:
                 layer = eidx[e, 3]
                 if f == 4 and layer == 0:
@@ -217,37 +218,26 @@ def _build_geometry(g: CubedSphereGrid) -> dict:
                     raise RuntimeError("unmatched interior face in the cubed-sphere grid")
                 continue
             e2, f2 = cands[0]
-            n2 = fnodes[f2].reshape(-1)
-            pts2 = xf[:, e2, n2]                   # (3, Nfp)
-            for jj in range(Nfp):
-                dist = np.sum((pts2 - xf[:, e, nf[jj]][:, None]) ** 2, axis=0)
-                kk = int(np.argmin(dist))
-                if dist[kk] > (1e-9 * scale) ** 2:
-                    raise RuntimeError("face nodes of neighbouring elements do not coincide")
-                nbr_node[e, f, jj] = e2 * Np + n2[kk]
+            d2 = np.sum((fx[:, e, f, :, None] - fx[:, e2, f2, None, :]) ** 2, axis=0)  # (Nfp, Nfp)
+            jj = np.argmin(d2, axis=1)
+            if np.max(d2[np.arange(Nfp), jj]) > (1e-9 * scale) ** 2:
+                raise RuntimeError("face nodes of neighbouring elements do not coincide")
+            nbr_node[e, f] = e2 * Np + fn_all[f2, jj]
+            partner[e, f] = (e2 * 6 + f2) * Nfp + jj
     # the two sides of an interior face share one normal (up to sign) and one
     # face mass, so the surface fluxes cancel exactly (conservation)
-    inv = [{int(n): j for j, n in enumerate(fnodes[f].reshape(-1))} for f in range(6)]
-    for e in range(K):
-        for f in range(6):
-            if btag[e, f]:
-                continue
-            for jj in range(Nfp):
-                e2, n2 = divmod(int(nbr_node[e, f, jj]), Np)
-                f2 = f ^ 1 if e2 != e else f  # matching face of the neighbour
-                for cand in range(6):
-                    if n2 in inv[cand] and not btag[e2, cand] and \
-                            nbr_node[e2, cand, inv[cand][n2]] == e * Np + fnodes[f].reshape(-1)[jj]:
-                        f2 = cand
-                        break
-                j2 = inv[f2][n2]
-                if (e2, f2, j2) < (e, f, jj):
-                    continue
-                nrm = normals[e, f, jj] - normals[e2, f2, j2]
-                nrm = nrm / np.sqrt(np.sum(nrm * nrm))
-                normals[e, f, jj], normals[e2, f2, j2] = nrm, -nrm
-                m = (fMJ[e, f, jj] + fMJ[e2, f2, j2]) / 2
-                fMJ[e, f, jj] = fMJ[e2, f2, j2] = m
+    pf = partner.reshape(-1)
+    nflat, mflat = normals.reshape(-1, 3), fMJ.reshape(-1)
+    a = np.nonzero((pf >= 0) & (np.arange(pf.size) < pf))[0]
+    b = pf[a]
+    if not np.array_equal(pf[b], a):
+        raise RuntimeError("the face map of the cubed-sphere grid is not symmetric")
+    nrm = nflat[a] - nflat[b]
+    nrm = nrm / np.sqrt(np.sum(nrm * nrm, axis=1, keepdims=True))
+    nflat[a], nflat[b] = nrm, -nrm
+    m = (mflat[a] + mflat[b]) / 2
+    mflat[a] = m
+    mflat[b] = m
     return {
         "x": xf, "J": J.reshape(K, Np), "g": gm.reshape(3, 3, K, Np), "MJ": MJ.reshape(K, Np),
         "face_nodes": np.stack([fn.reshape(-1) for fn in fnodes]).astype(np.int32),

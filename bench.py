@@ -43,7 +43,8 @@ sys.path.insert(0, ROOT)
 # (EC volume flux, Rusanov surface flux), from the oracle's instrumented
 # counter: python oracle/count_flops.py
 FLOPS_PER_DOF_STAGE = {"bubble_3d_N4_ec_rusanov": 602.8, "bubble_3d_N7_ec_rusanov": 896.2,
-                       "bubble_3d_N4_linear_weak_z": 22.4, "bubble_3d_N7_linear_weak_z": 25.1}
+                       "bubble_3d_N4_linear_weak_z": 22.4, "bubble_3d_N7_linear_weak_z": 25.1,
+                       "sphere_N5_ec_rusanov": 736.5, "sphere_N5_linear_weak_z": 22.9}
 L2_BYTES = 126 * 2 ** 20
 
 
@@ -848,7 +849,170 @@ def run_c5(args):
     return 0
 
 
-# ------------------------------------------- batched shallow-water instances# ------------------------------------------- batched shallow-water instances
+# ------------------------------------------------------ cubed-sphere shell
+def run_sphere(args):
+    """Acoustic wave on an Earth-radius cubed-sphere shell in the reference's
+    own configuration (experiment/euler_gravity/acousticwave.jl: N = 5,
+    KH = 10, KV = 5: 3000 curved hexahedra, 648,000 nodes, 3.24 M DOFs, 10 km
+    deep), EC volume + Rusanov surface flux, IMEX ARK23 (split_rhs = false)
+    with the vertical acoustics in the banded column solve (one band per
+    vertical line of nodes: the columns of a sphere differ), dt = 100 (H/KV) /
+    330 / N^2 (about 20 s).  Curved-element kernels: per-node metric terms, per
+    face-node normals, a node-level face map."""
+    import numpy as np
+    import torch
+
+    dist, rank, world = dist_init()
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    A = load_pkg()
+    from atum_b200 import _lib
+    from atum_b200 import workloads as P
+
+    N, KH, KV = 5, 10, 5
+    steps = args.steps if args.steps is not None else 20
+    t0 = time.perf_counter()
+    case = P.sphere_acoustic_wave(N=N, KH=KH, KV=KV, steps=steps)
+    t_setup = time.perf_counter() - t0
+    dofs = case.q0.size
+    L = _lib.lib()
+    stream = torch.cuda.current_stream()
+    q0 = torch.as_tensor(case.q0, device="cuda").contiguous()
+    q = q0.clone()
+    tuned = {"tendency": A.batch.autotune(case.dg, q), "tendency_linear": A.batch.autotune(case.lindg, q)}
+    t0 = time.perf_counter()
+    s = A.ARK23(case.dg, case.lindg, q, case.dt, split_rhs=False)
+    torch.cuda.synchronize()
+    t_solver = time.perf_counter() - t0
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    s.step(q, args.warmup)
+    q.copy_(q0)
+    barrier()
+    n0 = _lib.C.c_long()
+    L.atb_launch_count(_lib.C.byref(n0))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        barrier()
+        e0.record(stream)
+        s.step(q, steps)
+        e1.record(stream)
+        barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1), dist)
+    n1 = _lib.C.c_long()
+    L.atb_launch_count(_lib.C.byref(n1))
+    assert torch.isfinite(q).all(), "non-finite state after the timed steps"
+    _lib.check(L.atb_profile_reset())
+    _lib.check(L.atb_profile_enable(1))
+    qp = q.clone()
+    s.step(qp, 3)
+    barrier()
+    _lib.check(L.atb_profile_enable(0))
+    prof = {"steps": 3}
+    for k, name in enumerate(("tendency", "tendency_linear", "band_solve", "combine", "reduce")):
+        nl, tm = _lib.C.c_long(), _lib.C.c_double()
+        _lib.check(L.atb_profile_read(k, _lib.C.byref(nl), _lib.C.byref(tm)))
+        prof[name] = {"launches": nl.value, "ms": tm.value}
+    # mass drift over the timed steps (reflective shell: mass is conserved)
+    mj = torch.as_tensor(case.dg.MJ, device="cuda")
+    m0, m1 = float((q0[0] * mj).sum()), float((q[0] * mj).sum())
+
+    # e2e through the public API with host buffers (state in and out every step)
+    qh = torch.empty(case.q0.shape, dtype=torch.float64, pin_memory=True)
+    qh.copy_(torch.as_tensor(case.q0))
+    qd = torch.empty_like(q)
+    ke = max(3, min(steps, 20))
+    qd.copy_(qh, non_blocking=True)
+    s.step(qd, 1)
+    qh.copy_(qd, non_blocking=True)
+    barrier()
+    e0.record(stream)
+    for _ in range(ke):
+        qd.copy_(qh, non_blocking=True)
+        s.step(qd, 1)
+        qh.copy_(qd, non_blocking=True)
+    e1.record(stream)
+    barrier()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1), dist)
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+    peak_fp64 = _lib.C.c_double()
+    _lib.check(L.atb_probe_fp64_peak(_lib.C.byref(peak_fp64), _lib.stream_ptr()))
+    peaks, kind = measured_peaks()
+
+    def kern(name, flops_key, label):
+        t = prof[name]
+        if not t["launches"]:
+            return None
+        avg = t["ms"] / t["launches"]
+        fl = FLOPS_PER_DOF_STAGE[flops_key] * dofs
+        return {"kernel": label, "avg_launch_ms": avg, "bound": "fp64", "flops_per_dof_stage":
+                FLOPS_PER_DOF_STAGE[flops_key], "achieved_tflops": fl / (avg * 1e-3) / 1e12,
+                "peak_tflops": peak_fp64.value, "frac": fl / (avg * 1e-3) / 1e12 / peak_fp64.value}
+
+    value = world * dofs * 3 * steps / (ms * 1e-3)
+    tend = kern("tendency", "sphere_N5_ec_rusanov", "curved_kernel<EulerGravity,EC> (explicit stage tendency)")
+    lin = kern("tendency_linear", "sphere_N5_linear_weak_z",
+               "curved_kernel<LinearEulerGravity,WEAK> (vertical linear operator + ARK accumulation)")
+    b = prof["band_solve"]
+    band = None
+    if b["launches"]:
+        avgb = b["ms"] / b["launches"]
+        # per-line factors: each line's band (nunk x (2 bw + 1)) is read once,
+        # the right-hand side read and the solution written
+        nlines = 6 * KH * KH * (N + 1) ** 2
+        nunk = KV * (N + 1) * 5
+        W = 2 * (5 * (N + 1) - 1) + 1
+        byt = (nlines * nunk * W + 2 * dofs) * 8
+        band = {"kernel": "band_solve (generic: one factor per vertical line)", "avg_launch_ms": avgb,
+                "bound": "hbm", "bytes_per_launch": byt, "achieved_gbs": byt / (avgb * 1e-3) / 1e9,
+                "peak_gbs": peaks["hbm_gbs"], "frac": byt / (avgb * 1e-3) / 1e9 / peaks["hbm_gbs"],
+                "peak_kind": kind}
+    line = {
+        "metric": "DOF-stage updates/s", "value": value, "unit": "DOF-stage/s", "n_gpus": world, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (the reference experiment's initial state)",
+        "config": {"workload": f"3-D Euler-gravity acoustic wave on a cubed-sphere shell, 6x{KH}x{KH}x{KV} curved "
+                               f"hexahedra, N={N} ({dofs} DOFs), EC volume + Rusanov surface flux, IMEX ARK23 "
+                               "split_rhs=false, per-line vertical banded solve",
+                   "dofs": dofs, "stages_per_step": 3, "dt_s": case.dt,
+                   "l2": f"working set ~{dofs * 8 * 30 / 1e9:.1f} GB (state, stages, metrics, bands) > 126 MB L2"},
+        "elements_per_cta": tuned, "gpu_launches": int(n1.value - n0.value),
+        "setup_s": {"grid_and_initial_state_host": t_setup, "solver_with_band_factor": t_solver},
+        "e2e": {"value": world * dofs * 3 * ke / (ms_e2e * 1e-3), "unit": "DOF-stage/s",
+                "h2d_bytes_per_step": dofs * 8, "d2h_bytes_per_step": dofs * 8, "steps": ke},
+        "roofline": tend and {"bound": "fp64", "kernel": tend["kernel"], "achieved": tend["achieved_tflops"],
+                              "peak": tend["peak_tflops"], "unit": "TFLOP/s", "frac": tend["frac"],
+                              "peak_source": "measured in this run: FP64 FMA probe (atb_probe_fp64_peak)",
+                              "flops_per_dof_stage": tend["flops_per_dof_stage"], "traffic": None},
+        "kernels": {"tendency": tend, "tendency_linear": lin, "band_solve": band, "launch_totals": prof},
+        "mass_drift": abs(m1 - m0) / m0,
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as orc
+        threads = os.cpu_count() or 1
+        orc.set_threads(threads)
+        qo = case.q0.copy()
+        so = orc.ARK23(orc.DGSEM(case.dg), orc.DGSEM(case.lindg), qo, case.dt, split_rhs=False)
+        so.step(qo, 1)
+        n, T = _time_steps(so, qo, 10.0, 50)
+        line["cpu_baseline"] = {"value": dofs * 3 * n / T, "unit": "DOF-stage/s", "cores": threads, "kind": "port",
+                                "sample": f"{n} ARK23 steps of the same sphere workload, {threads} threads, "
+                                          f"{T:.1f} s"}
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+# ------------------------------------------- batched shallow-water instances
 def run_swbatch(args):
     """256 rotating shallow-water instances (f-plane, g = 9.81), each a
     periodic 32 x 32 square of N = 4 elements with its own seeded bathymetry
@@ -1009,7 +1173,7 @@ def main():
     ap.add_argument("--scheme", default="ark23", choices=sorted(SCHEME_STAGES),
                     help="time stepper of the bubble workload: IMEX ARK23 (default) or the fully explicit LSRK54 "
                          "run of the same problem")
-    ap.add_argument("--workload", default="bubble", choices=["bubble", "swbatch", "serve", "c5"],
+    ap.add_argument("--workload", default="bubble", choices=["bubble", "swbatch", "serve", "c5", "sphere"],
                     help="bubble: 3-D rising bubble, IMEX ARK23 (default); swbatch: packed shallow-water "
                          "instances; serve: Poisson request stream through the serving loop; c5: 128x128x32 "
                          "hexahedra at N=7, FP64 and FP32-flux")
@@ -1031,6 +1195,8 @@ def main():
         return run_swbatch(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "sphere":
+        return run_sphere(args)
     if args.workload == "c5":
         return run_c5(args)
     if args.steps is None:

@@ -80,6 +80,15 @@ def main():
     a = c5.dg.auxstate_host()
     out["bubble_3d_N7_ec_rusanov"] = fd_flops(c5.dg, 2, 1, x[:, 0, 0], a[:, 0, 0], x[:, 1, 9], a[:, 1, 9])
     out["bubble_3d_N7_linear_weak_z"] = weak_flops(c5.lindg, 1, x[:, 0, 0], a[:, 0, 0], x[:, 1, 9], a[:, 1, 9])
+    # cubed-sphere acoustic wave, N = 5 (the reference's contraction is the
+    # curved-element one already: all three two-point flux rows with both
+    # nodes' metric terms, so curvature changes no count)
+    from atum_b200 import workloads as W
+    sp = W.sphere_acoustic_wave(N=5, KH=1, KV=1, steps=1)
+    x = sp.q0
+    a = sp.dg.auxstate_host()
+    out["sphere_N5_ec_rusanov"] = fd_flops(sp.dg, 2, 1, x[:, 0, 0], a[:, 0, 0], x[:, 1, 9], a[:, 1, 9])
+    out["sphere_N5_linear_weak_z"] = weak_flops(sp.lindg, 1, x[:, 0, 0], a[:, 0, 0], x[:, 1, 9], a[:, 1, 9])
     print(json.dumps(out, indent=1, sort_keys=True))
 
 
