@@ -1028,6 +1028,7 @@ struct atb_solver {
   // operator), when the two operators allow it (atb_solver_fuse)
   tend_launch_fn fused = nullptr;
   bool fuse_on = false;
+  int lines_sparse = 0;  // per-line factors couple elements through face nodes only
   // per-element time steps (LSRK over packed instances), or null; owned by
   // the solver (atb_solver_set_instance_dt) or by the caller
   double* d_dte = nullptr;
@@ -1196,6 +1197,18 @@ int build_band(atb_solver* s, cudaStream_t st) {
     if (rc) return rc;
     launch_band_factor(M.nunk, M.bw, M.nlines, s->band, W, M.nlines, scale, st);
     s->ld = M.nlines;
+    // the face-node coupling structure of every line's factor lets the solve
+    // skip the zero blocks (ATB_BAND_DENSE=1 keeps the full band)
+    int* d_bad = nullptr;
+    if ((rc = dalloc(&d_bad, 1))) return rc;
+    CK(cudaMemsetAsync(d_bad, 0, sizeof(int), st));
+    launch_band_lines_structure(M, s->band, d_bad, st);
+    int bad = 1;
+    CK(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    cudaFree(d_bad);
+    const char* dense = std::getenv("ATB_BAND_DENSE");
+    s->lines_sparse = (bad == 0 && !(dense && dense[0] == '1')) ? 1 : 0;
   } else {
     cudaFree(P);
     cudaFree(LP);
@@ -1465,6 +1478,7 @@ int ark_step_accumulated(atb_solver* s, double* const* q, cudaStream_t st) {
     B.blk = s->blk;
     B.frag = s->frag;
     B.ld = s->ld;
+    B.lines_sparse = s->lines_sparse;
     B.npairs = 0;
     B.dt = s->dt;
     for (int c = 0; c < 5; ++c) { B.q[c] = R[c]; B.out[c] = Qout[c]; }
@@ -1554,6 +1568,7 @@ int ark_step(atb_solver* s, double* const* q, cudaStream_t st) {
       B.blk = s->blk;
       B.frag = s->frag;
       B.ld = s->ld;
+      B.lines_sparse = s->lines_sparse;
       B.npairs = i;
       B.dt = s->dt;
       for (int k = 0; k < i; ++k) {

@@ -1011,7 +1011,158 @@ bool warp_solve_structure_ok(const double* blk_host, int KV, int BW1, int NS) {
 // Dispatch: the block-parallel form when the factor is shared and its
 // per-element inverses were prepared, else the register-window substitution
 // (shared factor), else the generic per-line kernel.
+namespace {
+
+// ------------------------------------------------ per-line factors
+// Vertical lines whose factors differ (curved grids: every column of a sphere
+// has its own metric terms).  One thread per line, the factor in the
+// line-fastest layout band[(r * W + k) * nlines + line] (coalesced across the
+// threads of a warp), the element-block recurrence with compile-time block
+// size BW1 = NQ * NS so that the previous / next block's values and the
+// current block's live in registers.  Sums run in the generic kernel's order
+// (increasing column), so the results are the generic kernel's; with SPARSE
+// the entries that the face-node coupling makes zero (the sub-diagonal block
+// of L outside its face rows and columns, the super-diagonal block of U
+// likewise; launch_band_lines_structure checks every line at setup) are not
+// read, which halves the bytes of a solve.
+// one row of the forward (FWD) or backward pass, then the next: compile-time
+// row indices keep every block value in a register
+template <int NQ, int NS, bool SPARSE, bool FWD, int I>
+__device__ __forceinline__ void lines_rows(const BandSolve& B, const double* __restrict__ row0, size_t ld,
+                                           size_t eoff, int nh, bool has_nb, const double (&nb)[NQ * NS],
+                                           double (&cur)[NQ * NS]) {
+  constexpr int BW1 = NQ * NS;
+  constexpr int BW = BW1 - 1;
+  constexpr int W = 2 * BW + 1;
+  if constexpr (I >= 0 && I < BW1) {
+    constexpr int s = I % NS, kv = I / NS;
+    const size_t g = eoff + (size_t)nh * kv;
+    const double* row = row0 + (size_t)I * W * ld;
+    if constexpr (FWD) {
+      double acc = B.q[s][g];
+#pragma unroll
+      for (int k = 0; k < 2; ++k)
+        if (k < B.npairs) acc = acc + B.dt * (B.a[k] * B.ex[k][s][g] + B.b[k] * B.im[k][s][g]);
+      if (has_nb) {
+#pragma unroll
+        for (int jp = I + 1; jp < BW1; ++jp) {
+          if (SPARSE && !(I < NS && jp >= BW1 - NS)) continue;
+          acc = acc - row[(size_t)(jp - I - 1) * ld] * nb[jp];
+        }
+      }
+#pragma unroll
+      for (int jp = 0; jp < I; ++jp) acc = acc - row[(size_t)(jp - I + BW) * ld] * cur[jp];
+      cur[I] = acc;
+      B.out[s][g] = acc;
+      lines_rows<NQ, NS, SPARSE, FWD, I + 1>(B, row0, ld, eoff, nh, has_nb, nb, cur);
+    } else {
+      double acc = B.out[s][g];
+#pragma unroll
+      for (int jp = I + 1; jp < BW1; ++jp) acc = acc - row[(size_t)(jp - I + BW) * ld] * cur[jp];
+      if (has_nb) {
+#pragma unroll
+        for (int jp = 0; jp < I; ++jp) {
+          if (SPARSE && !(I >= BW1 - NS && jp < NS)) continue;
+          acc = acc - row[(size_t)(2 * BW1 - 1 + jp - I) * ld] * nb[jp];
+        }
+      }
+      cur[I] = acc / row[(size_t)BW * ld];
+      B.out[s][g] = cur[I];
+      lines_rows<NQ, NS, SPARSE, FWD, I - 1>(B, row0, ld, eoff, nh, has_nb, nb, cur);
+    }
+  }
+}
+
+template <int NQ, int NS, bool SPARSE>
+__global__ void __launch_bounds__(64) band_solve_lines_kernel(const BandSolve B) {
+  constexpr int BW1 = NQ * NS;
+  constexpr int BW = BW1 - 1;
+  constexpr int W = 2 * BW + 1;
+  const LineMap& M = B.M;
+  const int line = blockIdx.x * blockDim.x + threadIdx.x;
+  if (line >= M.nlines) return;
+  const size_t ld = (size_t)M.nlines;
+  const double* __restrict__ band = B.band + line;
+  const int hn = line % M.nh;
+  const int e0 = M.e0[line];
+  const int KV = M.KV, nh = M.nh, Np = M.Np;
+  double nb[BW1], cur[BW1];
+#pragma unroll
+  for (int j = 0; j < BW1; ++j) nb[j] = cur[j] = 0.0;
+  // forward: L y = rhs (unit diagonal)
+  for (int ev = 0; ev < KV; ++ev) {
+    const size_t eoff = (size_t)(e0 + ev * M.estep) * Np + hn;
+    lines_rows<NQ, NS, SPARSE, true, 0>(B, band + (size_t)ev * BW1 * W * ld, ld, eoff, nh, ev > 0, nb, cur);
+#pragma unroll
+    for (int j = 0; j < BW1; ++j) nb[j] = cur[j];
+  }
+  // backward: U x = y
+#pragma unroll
+  for (int j = 0; j < BW1; ++j) nb[j] = 0.0;
+  for (int ev = KV - 1; ev >= 0; --ev) {
+    const size_t eoff = (size_t)(e0 + ev * M.estep) * Np + hn;
+    lines_rows<NQ, NS, SPARSE, false, BW1 - 1>(B, band + (size_t)ev * BW1 * W * ld, ld, eoff, nh, ev < KV - 1, nb,
+                                               cur);
+#pragma unroll
+    for (int j = 0; j < BW1; ++j) nb[j] = cur[j];
+  }
+}
+
+typedef void (*lines_fn)(const BandSolve& B, cudaStream_t st);
+template <int NQ, int NS, bool SPARSE> void lines_launch(const BandSolve& B, cudaStream_t st) {
+  band_solve_lines_kernel<NQ, NS, SPARSE><<<(B.M.nlines + 63) / 64, 64, 0, st>>>(B);
+}
+template <int NS, bool SPARSE> lines_fn pick_lines_sp(int nq) {
+  switch (nq) {
+    case 2: return lines_launch<2, NS, SPARSE>;
+    case 3: return lines_launch<3, NS, SPARSE>;
+    case 4: return lines_launch<4, NS, SPARSE>;
+    case 5: return lines_launch<5, NS, SPARSE>;
+    case 6: return lines_launch<6, NS, SPARSE>;
+    case 7: return lines_launch<7, NS, SPARSE>;
+    case 8: return lines_launch<8, NS, SPARSE>;
+  }
+  return nullptr;
+}
+template <int NS> lines_fn pick_lines(int nq, bool sparse) {
+  return sparse ? pick_lines_sp<NS, true>(nq) : pick_lines_sp<NS, false>(nq);
+}
+
+__global__ void band_lines_structure_kernel(const LineMap M, const double* band, int* count) {
+  const int BW1 = M.Nq * M.ns, BW = BW1 - 1, W = 2 * BW + 1, NS = M.ns;
+  const size_t total = (size_t)M.nlines * M.nunk * W;
+  int bad = 0;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const size_t rk = t / M.nlines;
+    const int r = (int)(rk / W), k = (int)(rk - (size_t)r * W);
+    const int i = r % BW1;
+    bool skip = false;
+    if (k <= BW1 - 2 - i) {  // previous element block, column jp = k + i + 1
+      const int jp = k + i + 1;
+      skip = !(i < NS && jp >= BW1 - NS);
+    } else if (k >= 2 * BW1 - 1 - i) {  // next element block, column jp = k + i - (2 BW1 - 1)
+      const int jp = k + i - (2 * BW1 - 1);
+      skip = !(i >= BW1 - NS && jp < NS);
+    }
+    if (skip && band[t] != 0.0) bad = 1;
+  }
+  if (bad) atomicAdd(count, 1);
+}
+
+}  // namespace
+
+void launch_band_lines_structure(const LineMap& M, const double* band, int* count, cudaStream_t st) {
+  band_lines_structure_kernel<<<148 * 8, 256, 0, st>>>(M, band, count);
+}
+
 void launch_band_solve(const BandSolve& B, cudaStream_t st) {
+  if (B.ld > 1 && B.ld == B.M.nlines && B.npairs <= 2 && (B.M.ns == 4 || B.M.ns == 5)) {
+    lines_fn f = B.M.ns == 4 ? pick_lines<4>(B.M.Nq, B.lines_sparse != 0) : pick_lines<5>(B.M.Nq, B.lines_sparse != 0);
+    if (f) {
+      f(B, st);
+      return;
+    }
+  }
   if (B.ld == 1 && B.frag && B.npairs == 0 && (B.M.ns == 4 || B.M.ns == 5)) {
     warp_fn w = B.M.ns == 4 ? pick_warp<4>(B.M.Nq) : pick_warp<5>(B.M.Nq);
     if (w && w(B, st)) return;

@@ -71,8 +71,14 @@ struct BandSolve {
   double* out[5];
   const double* blk;  // per-element [L^-1 | G | U^-1 | H] blocks (shared factor), or null
   const double* frag; // the same blocks in matrix-unit fragment order (launch_frag_prep), or null
+  // per-line factors (ld = nlines): 1 when every line's factor couples
+  // neighbouring elements through face nodes only (launch_band_lines_structure)
+  int lines_sparse;
 };
 void launch_band_solve(const BandSolve& B, cudaStream_t st);
+// number of entries of the per-line factors (ld = nlines) outside the
+// face-node coupling structure that are not zero, added to *count
+void launch_band_lines_structure(const LineMap& M, const double* band, int* count, cudaStream_t st);
 void launch_block_prep(const double* band, int KV, int BW1, double* blk, cudaStream_t st);
 // the per-element tiles of the warp-owned solve (band_solve_warp_kernel)
 size_t frag_doubles(int KV, int BW1, int NS);

@@ -963,13 +963,14 @@ def run_sphere(args):
     band = None
     if b["launches"]:
         avgb = b["ms"] / b["launches"]
-        # per-line factors: each line's band (nunk x (2 bw + 1)) is read once,
-        # the right-hand side read and the solution written
+        # per-line factors: every line reads its factor's nonzero structure
+        # once -- per element block the dense diagonal block (L and U, BW1^2)
+        # and the ns x ns face-coupling blocks of L below and U above it --
+        # and the right-hand side, writes y, reads it back and writes x
         nlines = 6 * KH * KH * (N + 1) ** 2
-        nunk = KV * (N + 1) * 5
-        W = 2 * (5 * (N + 1) - 1) + 1
-        byt = (nlines * nunk * W + 2 * dofs) * 8
-        band = {"kernel": "band_solve (generic: one factor per vertical line)", "avg_launch_ms": avgb,
+        BW1 = 5 * (N + 1)
+        byt = (nlines * (KV * BW1 * BW1 + 2 * (KV - 1) * 25) + 4 * dofs) * 8
+        band = {"kernel": "band_solve_lines_kernel<6,5,sparse> (one factor per vertical line)", "avg_launch_ms": avgb,
                 "bound": "hbm", "bytes_per_launch": byt, "achieved_gbs": byt / (avgb * 1e-3) / 1e9,
                 "peak_gbs": peaks["hbm_gbs"], "frac": byt / (avgb * 1e-3) / 1e9 / peaks["hbm_gbs"],
                 "peak_kind": kind}

@@ -381,3 +381,19 @@ def test_sphere_measures_match_oracle(orc):
     for p in (2, np.inf):
         assert A.weightednorm(case.dg, qd, p) == pytest.approx(orc.weightednorm(o, case.q0, p), rel=1e-13)
     assert A.entropyintegral(case.dg, qd) == pytest.approx(orc.entropyintegral(o, case.q0), rel=1e-12)
+
+
+@pytest.mark.gpu
+def test_sphere_line_solve_sparse_equals_dense(monkeypatch):
+    """The per-line banded solve that skips the factors' face-coupling zero
+    blocks gives the full-band solve's results bit for bit."""
+    case = W.sphere_zonal_flow(N=3, KH=2, KV=3, steps=3)
+    out = []
+    for dense in ("1", "0"):
+        monkeypatch.setenv("ATB_BAND_DENSE", dense)
+        q = PT.to_dev(case.q0)
+        s = A.ARK23(case.dg, case.lindg, q, case.dt, split_rhs=False)
+        s.step(q, 3)
+        out.append(PT.to_host(q))
+        del s
+    assert np.array_equal(out[0], out[1])
