@@ -671,7 +671,7 @@ extern "C" int atb_op_create_curved(const atb_op_desc* d, const double* aux_host
   atb_op* op = nullptr;
   int rc = op_create_impl(d, 1, &aux_host, &op, d->naux > 0 && !aux_host);
   if (rc) return rc;
-  tend_launch_fn fn = pick_launcher_curved(d->law, op->vk);
+  tend_launch_fn fn = pick_launcher_curved(d->law, op->vk, sf);
   if (!fn) {
     atb_op_destroy(op);
     return fail(ATB_ERR_INVALID, "curved elements: no kernel for law %d, volume flux %d", d->law, d->volume_flux);

@@ -46,6 +46,46 @@ __device__ __forceinline__ double wavespeed_n(const LawP& L, const double* n, co
   }
 }
 
+// All three rows of the entropy-conservative two-point flux with the pair's
+// averages, logarithmic means and reciprocal computed once (the same
+// arithmetic as ec_sym_dir row by row, plus the Euler-gravity fluctuation
+// -alpha (Phi1 - Phi2) with alpha = b_avg rho_log / (2 b1) on each row's own
+// momentum entry).  P: u (3), p, b, |u|^2, e, p/rho.
+template <int LAW>
+__device__ __forceinline__ void ec_rows(double gamma, double r1, const double* P1, double Phi1, double r2,
+                                        const double* P2, double Phi2, double (*F)[CNS]) {
+  const double rho_avg = (r1 + r2) / 2.0;
+  double ua[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) ua[c] = (P1[c] + P2[c]) / 2.0;
+  const double b1 = P1[4], b2 = P2[4];
+  const double b_avg = (b1 + b2) / 2.0;
+  const double u2_avg = (P1[5] + P2[5]) / 2.0;
+  const double rho_log = logavg_fast(r1, r2);
+  const double b_log = logavg_fast(b1, b2);
+  const double rinv = 1.0 / (b_avg * b_log);
+  const double pc = rho_avg * b_log * rinv / 2.0;
+  double c1 = b_avg * rinv / (2.0 * (gamma - 1.0)) - u2_avg / 2.0;
+  if (LAW == LAW_EG) c1 = c1 + (Phi1 + Phi2) / 2.0;
+  const double fl = (LAW == LAW_EG) ? (b_avg * rho_log / (2.0 * b1)) * (Phi1 - Phi2) : 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double ud = ua[d];
+    const double frd = ud * rho_log;
+    F[d][0] = frd;
+    double mu = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double m = ud * (ua[c] * rho_log);
+      if (c == d) m = m + pc;
+      F[d][1 + c] = m;
+      mu = (c == 0) ? m * ua[c] : mu + m * ua[c];
+    }
+    F[d][4] = c1 * frd + mu;
+    if (LAW == LAW_EG) F[d][1 + d] = F[d][1 + d] - fl;
+  }
+}
+
 // two-point volume flux rows (entropy conservative / Kennedy-Gruber /
 // central) of the ordered pair (1 = own node, 2 = partner)
 template <int LAW, int VK>
@@ -54,8 +94,7 @@ __device__ __forceinline__ void twopoint_rows(const LawP& L, const double* q1, c
                                               double (*F)[CNS]) {
   if constexpr (VK == VK_EC) {
     const double Phi1 = (LAW == LAW_EG) ? a1[0] : 0.0, Phi2 = (LAW == LAW_EG) ? a2[0] : 0.0;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) ec_dir<LAW, 3>(L.gamma, d, q1[0], P1, Phi1, q2[0], P2, Phi2, F[d]);
+    ec_rows<LAW>(L.gamma, q1[0], P1, Phi1, q2[0], P2, Phi2, F);
   } else if constexpr (VK == VK_KG) {
     const double Phi1 = (LAW == LAW_EG) ? a1[0] : 0.0, Phi2 = (LAW == LAW_EG) ? a2[0] : 0.0;
 #pragma unroll
@@ -256,7 +295,9 @@ template <int VK> struct CurvedX {
   static constexpr int v = (VK == VK_WEAK) ? 3 * CNS : NPreE<3>::v + 9;
 };
 
-template <int LAW, int VK>
+// SF >= 0: the surface flux kind as a compile-time constant (the kernel then
+// carries no other flux's code); SF < 0: the kind given at run time
+template <int LAW, int VK, int SF>
 __global__ void __launch_bounds__(512) curved_kernel(const TendArgs A) {
   constexpr int NS = CNS;
   constexpr int NA = NAuxMax<LAW, 3>::v;
@@ -364,7 +405,7 @@ __global__ void __launch_bounds__(512) curved_kernel(const TendArgs A) {
       for (int c = 0; c < NA; ++c) ap[c] = am[c];
     }
     double nf[NS];
-    surface_flux_n<LAW>(A.law, A.sflux, n, qm, am, qp, ap, nf);
+    surface_flux_n<LAW>(A.law, SF >= 0 ? SF : A.sflux, n, qm, am, qp, ap, nf);
     const double fm = A.fMJ[fj];
 #pragma unroll
     for (int s = 0; s < NS; ++s) slot[(face * Nfp + j) * NS + s] = fm * nf[s];
@@ -379,6 +420,7 @@ __global__ void __launch_bounds__(512) curved_kernel(const TendArgs A) {
 #pragma unroll
   for (int s = 0; s < NS; ++s) T[s] = -0.0;
   if ((A.dirs >> 2) & 1) add_sources<LAW, 3>(A.law, VK == VK_WEAK, qn, an, T);
+#pragma unroll
   for (int d = 0; d < 3; ++d) {
     if (!((A.dirs >> d) & 1)) continue;
     const int i = ijk[d];
@@ -486,15 +528,15 @@ __global__ void __launch_bounds__(512) curved_kernel(const TendArgs A) {
   }
 }
 
-template <int LAW, int VK>
+template <int LAW, int VK, int SF>
 void curved_launch(const TendArgs& A, int grid, int block, size_t smem, cudaStream_t st) {
   static size_t configured = 0;
   if (smem > 48 * 1024 && smem > configured) {
-    if (cudaFuncSetAttribute(curved_kernel<LAW, VK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
+    if (cudaFuncSetAttribute(curved_kernel<LAW, VK, SF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
         cudaSuccess)
       configured = smem;
   }
-  curved_kernel<LAW, VK><<<grid, block, smem, st>>>(A);
+  curved_kernel<LAW, VK, SF><<<grid, block, smem, st>>>(A);
 }
 
 }  // namespace
@@ -506,23 +548,26 @@ size_t curved_smem_bytes(int vk, int naux, int Nq, int E) {
   return sizeof(double) * ((size_t)((Nq * Nq + 1) & ~1) + per * E);
 }
 
-tend_launch_fn pick_launcher_curved(int law, int vk) {
+tend_launch_fn pick_launcher_curved(int law, int vk, int sflux) {
+  // Rusanov (the sphere experiments' surface flux) built in; every other
+  // surface flux through the run-time kind
+  const bool rus = sflux == F_RUSANOV;
   switch (law) {
     case LAW_EULER:
-      if (vk == VK_WEAK) return curved_launch<LAW_EULER, VK_WEAK>;
-      if (vk == VK_EC) return curved_launch<LAW_EULER, VK_EC>;
-      if (vk == VK_KG) return curved_launch<LAW_EULER, VK_KG>;
-      if (vk == VK_CENTRAL) return curved_launch<LAW_EULER, VK_CENTRAL>;
+      if (vk == VK_WEAK) return rus ? curved_launch<LAW_EULER, VK_WEAK, F_RUSANOV> : curved_launch<LAW_EULER, VK_WEAK, -1>;
+      if (vk == VK_EC) return rus ? curved_launch<LAW_EULER, VK_EC, F_RUSANOV> : curved_launch<LAW_EULER, VK_EC, -1>;
+      if (vk == VK_KG) return rus ? curved_launch<LAW_EULER, VK_KG, F_RUSANOV> : curved_launch<LAW_EULER, VK_KG, -1>;
+      if (vk == VK_CENTRAL) return curved_launch<LAW_EULER, VK_CENTRAL, -1>;
       break;
     case LAW_EG:
-      if (vk == VK_WEAK) return curved_launch<LAW_EG, VK_WEAK>;
-      if (vk == VK_EC) return curved_launch<LAW_EG, VK_EC>;
-      if (vk == VK_KG) return curved_launch<LAW_EG, VK_KG>;
-      if (vk == VK_CENTRAL) return curved_launch<LAW_EG, VK_CENTRAL>;
+      if (vk == VK_WEAK) return rus ? curved_launch<LAW_EG, VK_WEAK, F_RUSANOV> : curved_launch<LAW_EG, VK_WEAK, -1>;
+      if (vk == VK_EC) return rus ? curved_launch<LAW_EG, VK_EC, F_RUSANOV> : curved_launch<LAW_EG, VK_EC, -1>;
+      if (vk == VK_KG) return rus ? curved_launch<LAW_EG, VK_KG, F_RUSANOV> : curved_launch<LAW_EG, VK_KG, -1>;
+      if (vk == VK_CENTRAL) return curved_launch<LAW_EG, VK_CENTRAL, -1>;
       break;
     case LAW_LEG:
-      if (vk == VK_WEAK) return curved_launch<LAW_LEG, VK_WEAK>;
-      if (vk == VK_CENTRAL) return curved_launch<LAW_LEG, VK_CENTRAL>;
+      if (vk == VK_WEAK) return rus ? curved_launch<LAW_LEG, VK_WEAK, F_RUSANOV> : curved_launch<LAW_LEG, VK_WEAK, -1>;
+      if (vk == VK_CENTRAL) return curved_launch<LAW_LEG, VK_CENTRAL, -1>;
       break;
   }
   return nullptr;
