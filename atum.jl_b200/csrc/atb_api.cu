@@ -1029,6 +1029,7 @@ struct atb_solver {
   tend_launch_fn fused = nullptr;
   bool fuse_on = false;
   int lines_sparse = 0;  // per-line factors couple elements through face nodes only
+  double* lblk = nullptr;  // per-line factors by element block (warp-per-line solve)
   // per-element time steps (LSRK over packed instances), or null; owned by
   // the solver (atb_solver_set_instance_dt) or by the caller
   double* d_dte = nullptr;
@@ -1049,6 +1050,7 @@ void solver_free(atb_solver* s) {
   cudaFree(s->imK);
   cudaFree(s->d_e0);
   cudaFree(s->band);
+  cudaFree(s->lblk);
   cudaFree(s->blk);
   cudaFree(s->frag);
   if (s->own_dte) cudaFree(s->d_dte);
@@ -1209,6 +1211,15 @@ int build_band(atb_solver* s, cudaStream_t st) {
     cudaFree(d_bad);
     const char* dense = std::getenv("ATB_BAND_DENSE");
     s->lines_sparse = (bad == 0 && !(dense && dense[0] == '1')) ? 1 : 0;
+    // with that structure, and element blocks no wider than a warp, the
+    // warp-per-line solve reads the factors rearranged by element block
+    // (ATB_LINE_SOLVE=thread keeps the thread-per-line kernel)
+    const char* ls = std::getenv("ATB_LINE_SOLVE");
+    const size_t nlb = linewarp_doubles(M);
+    if (s->lines_sparse && nlb && !(ls && std::strcmp(ls, "thread") == 0)) {
+      if ((rc = dalloc(&s->lblk, nlb))) return rc;
+      launch_linewarp_prep(M, s->band, s->lblk, st);
+    }
   } else {
     cudaFree(P);
     cudaFree(LP);
@@ -1403,6 +1414,36 @@ int run_fused(atb_solver* s, double* const* Q, const ArkAcc& ark, cudaStream_t s
   const int naux = op->dim + 3;  // [Phi, grad Phi, rho_ref, p_ref] staged for both operators
   A.naux = naux;
   int E = op->E;
+  if (op->curved) {
+    // curved elements: the explicit operator's launch shape, no prefetch
+    while (E > 1 && curved_smem_bytes(op->vk, naux, op->Nq, E, true) > 200 * 1024) --E;
+    const size_t bytes = curved_smem_bytes(op->vk, naux, op->Nq, E, true);
+    if (bytes > 227 * 1024) return fail(ATB_ERR_INVALID, "element too large for the fused curved ARK stage kernel");
+    A.E = E;
+    A.pf = 0;
+    A.epi = EPI_ARK;
+    A.lin_law = s->lin->law;
+    A.lin_sflux = s->lin->sflux;
+    A.lin_dirs = s->lin->dirs;
+    for (int j = 0; j < 3; ++j) {
+      for (int c = 0; c < 5; ++c) { A.acc[j][c] = ark.acc[j][c]; A.accin[j][c] = ark.accin[j][c]; }
+      A.ca[j] = ark.ca[j];
+      A.cb[j] = ark.cb[j];
+    }
+    A.adt = ark.adt;
+    for (int c = 0; c < 5; ++c) {
+      A.q[c] = Q[c];
+      A.out[c] = Q[c];  // not read by the fused epilogue
+      A.out2[c] = nullptr;
+    }
+    const int grid = (op->K_active + E - 1) / E;
+    if (grid == 0) return ATB_OK;
+    {
+      ProfScope ps(ATB_PROF_TEND, st);
+      s->fused(A, grid, cta_threads(E, op->Np), bytes, st);
+    }
+    return check_launch("fused curved ARK stage");
+  }
   int pf = 0;
   for (int j = 0; j < 3; ++j) pf += (ark.acc[j][0] && ark.accin[j][0]) ? 1 : 0;
   // the compact layout of the Nq-specialised kernels (atb_tendency.cuh)
@@ -1479,6 +1520,7 @@ int ark_step_accumulated(atb_solver* s, double* const* q, cudaStream_t st) {
     B.frag = s->frag;
     B.ld = s->ld;
     B.lines_sparse = s->lines_sparse;
+    B.lines_blocks = s->lblk;
     B.npairs = 0;
     B.dt = s->dt;
     for (int c = 0; c < 5; ++c) { B.q[c] = R[c]; B.out[c] = Qout[c]; }
@@ -1569,6 +1611,7 @@ int ark_step(atb_solver* s, double* const* q, cudaStream_t st) {
       B.frag = s->frag;
       B.ld = s->ld;
       B.lines_sparse = s->lines_sparse;
+      B.lines_blocks = s->lblk;
       B.npairs = i;
       B.dt = s->dt;
       for (int k = 0; k < i; ++k) {
@@ -1777,10 +1820,12 @@ extern "C" int atb_solver_set_dt(atb_solver* s, double dt) {
 }
 
 // Can the explicit and the linear operator of this ARK23 solver run as one
-// kernel per stage?  Euler-gravity (3-D, EC or FP32-flux EC volume flux) with
-// the weak-form linear Euler-gravity operator along z only, on the same grid
-// (bitwise identical metrics and neighbours) with the same leading aux fields
-// [Phi, grad Phi, rho_ref, p_ref] (bitwise identical on the device).
+// kernel per stage?  Euler-gravity (3-D, EC or FP32-flux EC volume flux; on
+// curved elements EC or KG with Rusanov faces) with the weak-form linear
+// Euler-gravity operator along z (the radial direction) only, on the same grid
+// (bitwise identical metrics and neighbours, curved geometry included) with
+// the same leading aux fields [Phi, grad Phi, rho_ref, p_ref] (bitwise
+// identical on the device).
 int fusion_check(atb_solver* s, cudaStream_t st) {
   s->fused = nullptr;
   atb_op *R = s->rhs, *L = s->lin;
@@ -1788,10 +1833,11 @@ int fusion_check(atb_solver* s, cudaStream_t st) {
   if (R->law.kind != LAW_EG || L->law.kind != LAW_LEG || R->dim != 3 || L->vk != VK_WEAK) return ATB_OK;
   if (L->dirs != (1 << (R->dim - 1))) return ATB_OK;
   if (R->K != L->K || R->Np != L->Np || R->stacked != L->stacked) return ATB_OK;
-  if (R->curved || L->curved) return ATB_OK;  // the fused stage kernel has brick metrics
+  if (R->curved != L->curved) return ATB_OK;
   const int na = R->dim + 3;
   if (R->naux < na || L->naux < na) return ATB_OK;
-  tend_launch_fn f = pick_launcher_fused(R->dim, R->vk, R->Nq, R->sflux, L->sflux);
+  tend_launch_fn f = R->curved ? pick_launcher_curved_fused(R->vk, R->sflux, L->sflux)
+                               : pick_launcher_fused(R->dim, R->vk, R->Nq, R->sflux, L->sflux);
   if (!f) return ATB_OK;
   unsigned long long* d_cnt = nullptr;
   int rc;
@@ -1801,6 +1847,15 @@ int fusion_check(atb_solver* s, cudaStream_t st) {
   launch_count_diff(R->d_ginv, L->d_ginv, K * 3 * 2, d_cnt, st);
   launch_count_diff(R->d_J, L->d_J, K * 2, d_cnt, st);
   launch_count_diff(R->d_nbr, L->d_nbr, K * 6, d_cnt, st);
+  if (R->curved) {
+    // the same curved geometry: metric terms, M J, face normals, masses and map
+    const size_t KF = K * 6 * R->Nfp;
+    launch_count_diff(R->d_G, L->d_G, 9 * n * 2, d_cnt, st);
+    launch_count_diff(R->d_MJn, L->d_MJn, n * 2, d_cnt, st);
+    launch_count_diff(R->d_fnrm, L->d_fnrm, 3 * KF * 2, d_cnt, st);
+    launch_count_diff(R->d_fMJ, L->d_fMJ, KF * 2, d_cnt, st);
+    launch_count_diff(R->d_fnb, L->d_fnb, KF, d_cnt, st);
+  }
   for (int k = 0; k < na; ++k) launch_count_diff(R->d_aux + (size_t)k * n, L->d_aux + (size_t)k * n, n * 2, d_cnt, st);
   unsigned long long cnt = 1;
   cudaError_t e1 = cudaMemcpyAsync(&cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, st);

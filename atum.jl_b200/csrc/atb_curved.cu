@@ -110,6 +110,78 @@ __device__ __forceinline__ void twopoint_rows(const LawP& L, const double* q1, c
   }
 }
 
+// The two-point flux of an ordered pair contracted with two direction
+// vectors, f1 = sum_c l1_c F#[c][:] and f2 = sum_c l2_c F#[c][:], from one set
+// of pair means.  For the entropy-conservative flux the contraction with l is
+// (U = l . u_avg, f_rho = U rho_log):
+//   [f_rho, f_rho u_avg + (p_c - fl) l, f_rho (c1 + |u_avg|^2) + p_c U]
+// with p_c = rho_avg / (2 b_avg), c1 = 1/(2 (gamma-1) b_log) - |u|^2_avg / 2
+// (+ Phi_avg), and fl = b_avg rho_log / (2 b1) (Phi1 - Phi2) the Euler-gravity
+// fluctuation on the momentum; for Kennedy-Gruber
+//   [U rho_avg, U rho_avg u_avg + (p_avg - rho_avg (Phi1 - Phi2) / 2) l,
+//    U (rho_avg e_avg + p_avg)]
+// -- the rows of ec_rows / kg_dir summed with the weights l, in fewer operations.
+template <int LAW, int VK>
+__device__ __forceinline__ void pair_contract(const LawP& L, const double* q1, const double* a1, const double* P1,
+                                              const double* q2, const double* a2, const double* P2,
+                                              const double* l1, const double* l2, double* f1, double* f2) {
+  if constexpr (VK == VK_EC || VK == VK_KG) {
+    const double r1 = q1[0], r2 = q2[0];
+    const double Phi1 = (LAW == LAW_EG) ? a1[0] : 0.0, Phi2 = (LAW == LAW_EG) ? a2[0] : 0.0;
+    const double rho_avg = (r1 + r2) / 2.0;
+    double ua[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) ua[c] = (P1[c] + P2[c]) / 2.0;
+    double rho_m, pc, c4;  // momentum / energy coefficients
+    double fl = 0.0;
+    if constexpr (VK == VK_EC) {
+      const double b1 = P1[4], b2 = P2[4];
+      const double b_avg = (b1 + b2) / 2.0;
+      const double u2_avg = (P1[5] + P2[5]) / 2.0;
+      rho_m = logavg_fast(r1, r2);
+      const double b_log = logavg_fast(b1, b2);
+      const double rinv = 1.0 / (b_avg * b_log);
+      pc = rho_avg * b_log * rinv / 2.0;
+      double c1 = b_avg * rinv / (2.0 * (L.gamma - 1.0)) - u2_avg / 2.0;
+      if (LAW == LAW_EG) {
+        c1 = c1 + (Phi1 + Phi2) / 2.0;
+        fl = (b_avg * rho_m / (2.0 * b1)) * (Phi1 - Phi2);
+      }
+      c4 = c1 + dot<3>(ua, ua);
+    } else {
+      rho_m = rho_avg;
+      pc = (P1[3] + P2[3]) / 2.0;  // p_avg
+      c4 = rho_avg * ((P1[6] + P2[6]) / 2.0) + pc;  // rho_avg e_avg + p_avg
+      if (LAW == LAW_EG) fl = (rho_avg / 2.0) * (Phi1 - Phi2);
+    }
+    const double pm = pc - fl;
+    const double U1 = dot<3>(l1, ua), U2 = dot<3>(l2, ua);
+    const double fr1 = U1 * rho_m, fr2 = U2 * rho_m;
+    f1[0] = fr1;
+    f2[0] = fr2;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      f1[1 + k] = fr1 * ua[k] + pm * l1[k];
+      f2[1 + k] = fr2 * ua[k] + pm * l2[k];
+    }
+    if constexpr (VK == VK_EC) {
+      f1[4] = fr1 * c4 + pc * U1;
+      f2[4] = fr2 * c4 + pc * U2;
+    } else {
+      f1[4] = U1 * c4;
+      f2[4] = U2 * c4;
+    }
+  } else {
+    double F[3][CNS];
+    twopoint_rows<LAW, VK>(L, q1, a1, P1, q2, a2, P2, F);
+#pragma unroll
+    for (int s = 0; s < CNS; ++s) {
+      f1[s] = l1[0] * F[0][s] + l1[1] * F[1][s] + l1[2] * F[2][s];
+      f2[s] = l2[0] * F[0][s] + l2[1] * F[1][s] + l2[2] * F[2][s];
+    }
+  }
+}
+
 // boundarystate(law, problem, n, q-, aux-, tag) for a general normal
 __device__ __forceinline__ void boundary_state_n(const LawP& L, const double* n, int tag, const double* qm,
                                                  double* qp) {
@@ -296,8 +368,16 @@ template <int VK> struct CurvedX {
 };
 
 // SF >= 0: the surface flux kind as a compile-time constant (the kernel then
-// carries no other flux's code); SF < 0: the kind given at run time
-template <int LAW, int VK, int SF>
+// carries no other flux's code); SF < 0: the kind given at run time.
+// FUSE: one IMEX ARK23 stage (split_rhs = false) of Euler-gravity with the
+// weak-form linear Euler-gravity operator along the radial direction: the
+// explicit tendency N(Q), the linear operator L(Q) (its contravariant radial
+// flux rows staged beside the state, its faces in the same task loop, its
+// source) and the EPI_ARK accumulation of N - L and L in one launch, so the
+// state, aux fields and metric terms are read once per stage.  Per element
+// shared memory then adds NS * Np (linear flux rows) and 2 * Nfp * NS (linear
+// face slots); all six aux fields are staged.
+template <int LAW, int VK, int SF, bool FUSE = false>
 __global__ void __launch_bounds__(512) curved_kernel(const TendArgs A) {
   constexpr int NS = CNS;
   constexpr int NA = NAuxMax<LAW, 3>::v;
@@ -306,7 +386,8 @@ __global__ void __launch_bounds__(512) curved_kernel(const TendArgs A) {
   const int Nq = A.Nq, Np = A.Np, Nfp = A.Nfp, E = A.E, na = A.naux;
   const int nqq = (Nq * Nq + 1) & ~1;
   double* sD = smem;  // D[i][m] = l_m'(xi_i)
-  const size_t per = (size_t)(NS + na + NX) * Np + (size_t)6 * Nfp * NS;
+  const size_t per = (size_t)(NS + na + NX) * Np + (size_t)6 * Nfp * NS +
+                     (FUSE ? (size_t)NS * Np + (size_t)2 * Nfp * NS : 0);
   const int tid = threadIdx.x;
   const int el = tid / Np;
   const int node = tid - el * Np;
@@ -317,6 +398,8 @@ __global__ void __launch_bounds__(512) curved_kernel(const TendArgs A) {
   double* sq = base;
   double* sa = sq + (size_t)NS * Np;
   double* sx = sa + (size_t)na * Np;
+  // fused: linear radial flux rows after the face slots, then the linear face slots
+  double* sxl = sx + (size_t)NX * Np + (size_t)6 * Nfp * NS;
   const size_t stride = A.stride;
   const size_t gid = (size_t)e * Np + node;
   double qn[NS], an[NA];
@@ -334,10 +417,25 @@ __global__ void __launch_bounds__(512) curved_kernel(const TendArgs A) {
       sa[k * Np + node] = an[k];
     }
     MJ = A.MJn[gid];
+    // metric terms of the active directions only (the radial linear operator
+    // of the IMEX stages reads a third of them)
 #pragma unroll
     for (int d = 0; d < 3; ++d)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) lg[d][c] = A.G[((size_t)d * 3 + c) * stride + gid];
+      for (int c = 0; c < 3; ++c) lg[d][c] = ((A.dirs >> d) & 1) ? A.G[((size_t)d * 3 + c) * stride + gid] : 0.0;
+    if constexpr (FUSE) {
+      // the linear operator's contravariant radial flux rows (its volume
+      // term's staged values: MJ g[3, :] . F_lin), as the weak-form kernel
+      double F[3][NS];
+      flux_rows<LAW_LEG>(A.lin_law, qn, an, F);
+#pragma unroll
+      for (int s2 = 0; s2 < NS; ++s2) {
+        double acc = 0.0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc = acc + lg[2][c] * F[c][s2];
+        sxl[s2 * Np + node] = acc * MJ;
+      }
+    }
     if constexpr (VK == VK_WEAK) {
       double F[3][NS];
       flux_rows<LAW>(A.law, qn, an, F);
@@ -409,6 +507,15 @@ __global__ void __launch_bounds__(512) curved_kernel(const TendArgs A) {
     const double fm = A.fMJ[fj];
 #pragma unroll
     for (int s = 0; s < NS; ++s) slot[(face * Nfp + j) * NS + s] = fm * nf[s];
+    if constexpr (FUSE) {
+      if (k == 2) {  // the linear operator's radial faces
+        double* sl = fb + (size_t)(NS + na + NX) * Np + (size_t)6 * Nfp * NS + (size_t)NS * Np;
+        if (nb < 0) boundary_state_n(A.lin_law, n, -1 - nb, qm, qp);
+        surface_flux_n<LAW_LEG>(A.lin_law, A.lin_sflux, n, qm, am, qp, ap, nf);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) sl[(side * Nfp + j) * NS + s] = fm * nf[s];
+      }
+    }
   }
   __syncthreads();
   if (!active) return;
@@ -450,16 +557,11 @@ __global__ void __launch_bounds__(512) curved_kernel(const TendArgs A) {
         for (int k = 0; k < NPreE<3>::v; ++k) P2[k] = sx[k * Np + nn];
 #pragma unroll
         for (int c = 0; c < 3; ++c) lm[c] = sx[(NPreE<3>::v + d * 3 + c) * Np + nn];
-        double F[3][NS];
-        twopoint_rows<LAW, VK>(A.law, qn, an, P1, q2, a2, P2, F);
+        double f1[NS], f2[NS];
+        pair_contract<LAW, VK>(A.law, qn, an, P1, q2, a2, P2, lg[d], lm, f1, f2);
         const double Ddn = MJI * sD[i * Nq + m], Dnd = MJI * sD[m * Nq + i];
 #pragma unroll
-        for (int s = 0; s < NS; ++s)
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            T[s] = T[s] - Ddn * lg[d][c] * F[c][s];
-            T[s] = T[s] + F[c][s] * lm[c] * Dnd;
-          }
+        for (int s = 0; s < NS; ++s) T[s] = T[s] - Ddn * f1[s] + Dnd * f2[s];
       }
     }
   }
@@ -475,6 +577,40 @@ __global__ void __launch_bounds__(512) curved_kernel(const TendArgs A) {
     const int face = 2 * k + side;
 #pragma unroll
     for (int s = 0; s < NS; ++s) T[s] = T[s] - slot[(face * Nfp + j) * NS + s] * MJI;
+  }
+  // fused: the linear operator L(Q) along the radial direction (the weak-form
+  // kernel's sums in its order: source, D^T of the staged rows, faces)
+  double TL[NS];
+  if constexpr (FUSE) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) TL[s] = -0.0;
+    add_sources<LAW_LEG, 3>(A.lin_law, true, qn, an, TL);
+    const int i = ijk[2];
+    const int n0 = node - i * Nq * Nq;
+    for (int m = 0; m < Nq; ++m) {
+      const double Dm = sD[m * Nq + i] * MJI;
+      const int nn = n0 + m * Nq * Nq;
+#pragma unroll
+      for (int s = 0; s < NS; ++s) TL[s] = TL[s] + Dm * sxl[s * Np + nn];
+    }
+    if (i == 0 || i == Nq - 1) {
+      const double* sl = sxl + (size_t)NS * Np;
+      const int side = (i == Nq - 1) ? 1 : 0;
+      const int j = ijk[0] + Nq * ijk[1];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) TL[s] = TL[s] - sl[(side * Nfp + j) * NS + s] * MJI;
+    }
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const double Ex = T[s] - TL[s];
+#pragma unroll
+      for (int jj = 0; jj < 3; ++jj)
+        if (A.acc[jj][0]) {
+          const double b0 = A.accin[jj][0] ? A.accin[jj][s][gid] : qn[s];
+          A.acc[jj][s][gid] = b0 + A.adt * (A.ca[jj] * Ex + A.cb[jj] * TL[s]);
+        }
+    }
+    return;
   }
 
   // ----------------------------------------------------------- epilogue
@@ -528,24 +664,34 @@ __global__ void __launch_bounds__(512) curved_kernel(const TendArgs A) {
   }
 }
 
-template <int LAW, int VK, int SF>
+template <int LAW, int VK, int SF, bool FUSE = false>
 void curved_launch(const TendArgs& A, int grid, int block, size_t smem, cudaStream_t st) {
   static size_t configured = 0;
   if (smem > 48 * 1024 && smem > configured) {
-    if (cudaFuncSetAttribute(curved_kernel<LAW, VK, SF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
-        cudaSuccess)
+    if (cudaFuncSetAttribute(curved_kernel<LAW, VK, SF, FUSE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) == cudaSuccess)
       configured = smem;
   }
-  curved_kernel<LAW, VK, SF><<<grid, block, smem, st>>>(A);
+  curved_kernel<LAW, VK, SF, FUSE><<<grid, block, smem, st>>>(A);
 }
 
 }  // namespace
 
-size_t curved_smem_bytes(int vk, int naux, int Nq, int E) {
+size_t curved_smem_bytes(int vk, int naux, int Nq, int E, bool fuse) {
   const int Np = Nq * Nq * Nq, Nfp = Nq * Nq;
   const int nx = (vk == VK_WEAK) ? 3 * CNS : NPreE<3>::v + 9;
-  const size_t per = (size_t)(CNS + naux + nx) * Np + (size_t)6 * Nfp * CNS;
+  size_t per = (size_t)(CNS + naux + nx) * Np + (size_t)6 * Nfp * CNS;
+  if (fuse) per += (size_t)CNS * Np + (size_t)2 * Nfp * CNS;
   return sizeof(double) * ((size_t)((Nq * Nq + 1) & ~1) + per * E);
+}
+
+tend_launch_fn pick_launcher_curved_fused(int vk, int sflux, int lin_sflux) {
+  // Euler-gravity with the EC or KG volume flux and the Rusanov flux on both
+  // operators' faces (the sphere experiments); nullptr otherwise
+  if (sflux != F_RUSANOV || lin_sflux != F_RUSANOV) return nullptr;
+  if (vk == VK_EC) return curved_launch<LAW_EG, VK_EC, F_RUSANOV, true>;
+  if (vk == VK_KG) return curved_launch<LAW_EG, VK_KG, F_RUSANOV, true>;
+  return nullptr;
 }
 
 tend_launch_fn pick_launcher_curved(int law, int vk, int sflux) {

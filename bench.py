@@ -945,19 +945,25 @@ def run_sphere(args):
     _lib.check(L.atb_probe_fp64_peak(_lib.C.byref(peak_fp64), _lib.stream_ptr()))
     peaks, kind = measured_peaks()
 
-    def kern(name, flops_key, label):
+    def kern(name, flops_keys, label):
         t = prof[name]
         if not t["launches"]:
             return None
         avg = t["ms"] / t["launches"]
-        fl = FLOPS_PER_DOF_STAGE[flops_key] * dofs
-        return {"kernel": label, "avg_launch_ms": avg, "bound": "fp64", "flops_per_dof_stage":
-                FLOPS_PER_DOF_STAGE[flops_key], "achieved_tflops": fl / (avg * 1e-3) / 1e12,
+        fpd = sum(FLOPS_PER_DOF_STAGE[k] for k in flops_keys)
+        fl = fpd * dofs
+        return {"kernel": label, "avg_launch_ms": avg, "bound": "fp64", "flops_per_dof_stage": fpd,
+                "achieved_tflops": fl / (avg * 1e-3) / 1e12,
                 "peak_tflops": peak_fp64.value, "frac": fl / (avg * 1e-3) / 1e12 / peak_fp64.value}
 
     value = world * dofs * 3 * steps / (ms * 1e-3)
-    tend = kern("tendency", "sphere_N5_ec_rusanov", "curved_kernel<EulerGravity,EC> (explicit stage tendency)")
-    lin = kern("tendency_linear", "sphere_N5_linear_weak_z",
+    # the stage kernel: the explicit EC tendency, fused with the radial linear
+    # operator and the ARK accumulation when the solver fuses them
+    fused = prof["tendency_linear"]["launches"] == 0
+    tend = kern("tendency", ["sphere_N5_ec_rusanov"] + (["sphere_N5_linear_weak_z"] if fused else []),
+                "curved_kernel<EulerGravity,EC,Rusanov,fused> (ARK23 stage: EC tendency + radial linear operator)"
+                if fused else "curved_kernel<EulerGravity,EC> (explicit stage tendency)")
+    lin = kern("tendency_linear", ["sphere_N5_linear_weak_z"],
                "curved_kernel<LinearEulerGravity,WEAK> (vertical linear operator + ARK accumulation)")
     b = prof["band_solve"]
     band = None
