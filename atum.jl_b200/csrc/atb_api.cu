@@ -1029,7 +1029,6 @@ struct atb_solver {
   tend_launch_fn fused = nullptr;
   bool fuse_on = false;
   int lines_sparse = 0;  // per-line factors couple elements through face nodes only
-  double* lblk = nullptr;  // per-line factors by element block (warp-per-line solve)
   // per-element time steps (LSRK over packed instances), or null; owned by
   // the solver (atb_solver_set_instance_dt) or by the caller
   double* d_dte = nullptr;
@@ -1050,7 +1049,6 @@ void solver_free(atb_solver* s) {
   cudaFree(s->imK);
   cudaFree(s->d_e0);
   cudaFree(s->band);
-  cudaFree(s->lblk);
   cudaFree(s->blk);
   cudaFree(s->frag);
   if (s->own_dte) cudaFree(s->d_dte);
@@ -1211,15 +1209,6 @@ int build_band(atb_solver* s, cudaStream_t st) {
     cudaFree(d_bad);
     const char* dense = std::getenv("ATB_BAND_DENSE");
     s->lines_sparse = (bad == 0 && !(dense && dense[0] == '1')) ? 1 : 0;
-    // with that structure, and element blocks no wider than a warp, the
-    // warp-per-line solve reads the factors rearranged by element block
-    // (ATB_LINE_SOLVE=thread keeps the thread-per-line kernel)
-    const char* ls = std::getenv("ATB_LINE_SOLVE");
-    const size_t nlb = linewarp_doubles(M);
-    if (s->lines_sparse && nlb && !(ls && std::strcmp(ls, "thread") == 0)) {
-      if ((rc = dalloc(&s->lblk, nlb))) return rc;
-      launch_linewarp_prep(M, s->band, s->lblk, st);
-    }
   } else {
     cudaFree(P);
     cudaFree(LP);
@@ -1520,7 +1509,6 @@ int ark_step_accumulated(atb_solver* s, double* const* q, cudaStream_t st) {
     B.frag = s->frag;
     B.ld = s->ld;
     B.lines_sparse = s->lines_sparse;
-    B.lines_blocks = s->lblk;
     B.npairs = 0;
     B.dt = s->dt;
     for (int c = 0; c < 5; ++c) { B.q[c] = R[c]; B.out[c] = Qout[c]; }
@@ -1611,7 +1599,6 @@ int ark_step(atb_solver* s, double* const* q, cudaStream_t st) {
       B.frag = s->frag;
       B.ld = s->ld;
       B.lines_sparse = s->lines_sparse;
-      B.lines_blocks = s->lblk;
       B.npairs = i;
       B.dt = s->dt;
       for (int k = 0; k < i; ++k) {

@@ -1128,140 +1128,6 @@ template <int NS> lines_fn pick_lines(int nq, bool sparse) {
   return sparse ? pick_lines_sp<NS, true>(nq) : pick_lines_sp<NS, false>(nq);
 }
 
-// ------------------------------------------- per-line factors, one warp per line
-// The same solve with a warp per line and the factor rearranged per element
-// block: the in-place LU of the diagonal block column-major (L strictly below,
-// U on and above the diagonal) and the NS x NS face-coupling blocks of L (rows
-// 0..NS-1, the previous block's last NS columns) and U (rows BW1-NS..BW1-1,
-// the next block's first NS columns).  Lane i owns row i of the block (BW1 <=
-// 32); the substitutions run column by column: the value of column j is taken
-// from lane j by a shuffle and every later row subtracts its entry times it,
-// so each step is one shuffle and one multiply-add on the dependence chain and
-// a warp reads each column as one coalesced load.  Forward sums run in the
-// per-line kernel's order (coupling block first, then increasing columns);
-// backward sums run from the next block's coupling block down the columns.
-template <int NQ, int NS>
-__global__ void __launch_bounds__(256) band_solve_linewarp_kernel(const BandSolve B, const double* __restrict__ blocks) {
-  constexpr int BW1 = NQ * NS;
-  constexpr int BLK = BW1 * BW1 + 2 * NS * NS;
-  static_assert(BW1 <= 32, "one lane per row");
-  const LineMap& M = B.M;
-  const int lane = threadIdx.x & 31;
-  const int line = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (line >= M.nlines) return;  // the whole warp leaves together
-  const bool row = lane < BW1;
-  const int s = row ? lane % NS : 0, kv = row ? lane / NS : 0;
-  const int hn = line % M.nh, e0 = M.e0[line], KV = M.KV;
-  const double* __restrict__ lb = blocks + (size_t)line * KV * BLK;
-  constexpr unsigned FULL = 0xffffffffu;
-  double nb[NS];
-#pragma unroll
-  for (int k = 0; k < NS; ++k) nb[k] = 0.0;
-  // forward: L y = rhs
-  for (int ev = 0; ev < KV; ++ev) {
-    const double* bl = lb + (size_t)ev * BLK;
-    const size_t g = (size_t)(e0 + ev * M.estep) * M.Np + hn + (size_t)M.nh * kv;
-    double col[BW1];
-#pragma unroll
-    for (int j = 0; j < BW1; ++j) col[j] = row ? bl[j * BW1 + lane] : 0.0;
-    double acc = 0.0;
-    if (row) {
-      acc = B.q[s][g];
-#pragma unroll
-      for (int k = 0; k < 2; ++k)
-        if (k < B.npairs) acc = acc + B.dt * (B.a[k] * B.ex[k][s][g] + B.b[k] * B.im[k][s][g]);
-      if (ev > 0 && lane < NS) {
-#pragma unroll
-        for (int jp = 0; jp < NS; ++jp) acc = acc - bl[BW1 * BW1 + lane * NS + jp] * nb[jp];
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < BW1 - 1; ++j) {
-      const double yj = __shfl_sync(FULL, acc, j);
-      if (lane > j) acc = acc - col[j] * yj;
-    }
-    if (row) B.out[s][g] = acc;
-#pragma unroll
-    for (int k = 0; k < NS; ++k) nb[k] = __shfl_sync(FULL, acc, BW1 - NS + k);
-  }
-  // backward: U x = y
-#pragma unroll
-  for (int k = 0; k < NS; ++k) nb[k] = 0.0;
-  for (int ev = KV - 1; ev >= 0; --ev) {
-    const double* bl = lb + (size_t)ev * BLK;
-    const size_t g = (size_t)(e0 + ev * M.estep) * M.Np + hn + (size_t)M.nh * kv;
-    double col[BW1];
-#pragma unroll
-    for (int j = 0; j < BW1; ++j) col[j] = row ? bl[j * BW1 + lane] : 1.0;
-    double acc = row ? B.out[s][g] : 0.0;
-    if (row && ev < KV - 1 && lane >= BW1 - NS) {
-#pragma unroll
-      for (int jp = 0; jp < NS; ++jp)
-        acc = acc - bl[BW1 * BW1 + NS * NS + (lane - (BW1 - NS)) * NS + jp] * nb[jp];
-    }
-#pragma unroll
-    for (int j = BW1 - 1; j >= 0; --j) {
-      if (lane == j) acc = acc / col[j];
-      const double xj = __shfl_sync(FULL, acc, j);
-      if (lane < j) acc = acc - col[j] * xj;
-    }
-    if (row) B.out[s][g] = acc;
-#pragma unroll
-    for (int k = 0; k < NS; ++k) nb[k] = __shfl_sync(FULL, acc, k);
-  }
-}
-
-// blocks[(line * KV + ev) * BLK + e] from the per-line band factor
-__global__ void linewarp_prep_kernel(const LineMap M, const double* band, double* blocks) {
-  const int BW1 = M.Nq * M.ns, NS = M.ns, BW = BW1 - 1, W = 2 * BW + 1;
-  const int BLK = BW1 * BW1 + 2 * NS * NS;
-  const size_t total = (size_t)M.nlines * M.KV * BLK;
-  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
-    const int e = (int)(t % BLK);
-    const size_t le = t / BLK;
-    const int ev = (int)(le % M.KV);
-    const int line = (int)(le / M.KV);
-    int i, k;
-    bool zero = false;
-    if (e < BW1 * BW1) {  // diagonal block, column-major: entry (i, j) at j * BW1 + i
-      const int j = e / BW1;
-      i = e - j * BW1;
-      k = j - i + BW;
-    } else if (e < BW1 * BW1 + NS * NS) {  // L coupling (i, BW1 - NS + jp) of the previous block
-      const int c = e - BW1 * BW1;
-      i = c / NS;
-      const int jp = c - i * NS;
-      k = BW1 - NS + jp - i - 1;
-      zero = ev == 0;
-    } else {  // U coupling (BW1 - NS + ip, jp) of the next block
-      const int c = e - BW1 * BW1 - NS * NS;
-      const int ip = c / NS, jp = c - ip * NS;
-      i = BW1 - NS + ip;
-      k = 2 * BW1 - 1 + jp - i;
-      zero = ev == M.KV - 1;
-    }
-    const size_t r = (size_t)ev * BW1 + i;
-    blocks[t] = zero ? 0.0 : band[(r * W + k) * M.nlines + line];
-  }
-}
-
-typedef void (*linewarp_fn)(const BandSolve& B, const double* blocks, cudaStream_t st);
-template <int NQ, int NS> void linewarp_launch(const BandSolve& B, const double* blocks, cudaStream_t st) {
-  band_solve_linewarp_kernel<NQ, NS><<<(B.M.nlines + 7) / 8, 256, 0, st>>>(B, blocks);
-}
-template <int NS> linewarp_fn pick_linewarp(int nq) {
-  switch (nq) {
-    case 2: return linewarp_launch<2, NS>;
-    case 3: return linewarp_launch<3, NS>;
-    case 4: return linewarp_launch<4, NS>;
-    case 5: return linewarp_launch<5, NS>;
-    case 6: return linewarp_launch<6, NS>;
-    case 7: return NS * 7 <= 32 ? linewarp_launch<7, (NS * 7 <= 32 ? NS : 4)> : nullptr;
-    case 8: return NS * 8 <= 32 ? linewarp_launch<8, (NS * 8 <= 32 ? NS : 4)> : nullptr;
-  }
-  return nullptr;
-}
-
 __global__ void band_lines_structure_kernel(const LineMap M, const double* band, int* count) {
   const int BW1 = M.Nq * M.ns, BW = BW1 - 1, W = 2 * BW + 1, NS = M.ns;
   const size_t total = (size_t)M.nlines * M.nunk * W;
@@ -1289,24 +1155,7 @@ void launch_band_lines_structure(const LineMap& M, const double* band, int* coun
   band_lines_structure_kernel<<<148 * 8, 256, 0, st>>>(M, band, count);
 }
 
-size_t linewarp_doubles(const LineMap& M) {
-  const int BW1 = M.Nq * M.ns;
-  if (BW1 > 32 || (M.ns != 4 && M.ns != 5)) return 0;
-  return (size_t)M.nlines * M.KV * (BW1 * BW1 + 2 * M.ns * M.ns);
-}
-
-void launch_linewarp_prep(const LineMap& M, const double* band, double* blocks, cudaStream_t st) {
-  linewarp_prep_kernel<<<148 * 16, 256, 0, st>>>(M, band, blocks);
-}
-
 void launch_band_solve(const BandSolve& B, cudaStream_t st) {
-  if (B.lines_blocks && B.ld > 1 && B.ld == B.M.nlines && B.npairs <= 2 && (B.M.ns == 4 || B.M.ns == 5)) {
-    linewarp_fn f = B.M.ns == 4 ? pick_linewarp<4>(B.M.Nq) : pick_linewarp<5>(B.M.Nq);
-    if (f) {
-      f(B, B.lines_blocks, st);
-      return;
-    }
-  }
   if (B.ld > 1 && B.ld == B.M.nlines && B.npairs <= 2 && (B.M.ns == 4 || B.M.ns == 5)) {
     lines_fn f = B.M.ns == 4 ? pick_lines<4>(B.M.Nq, B.lines_sparse != 0) : pick_lines<5>(B.M.Nq, B.lines_sparse != 0);
     if (f) {

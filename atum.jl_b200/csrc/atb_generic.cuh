@@ -74,18 +74,11 @@ struct BandSolve {
   // per-line factors (ld = nlines): 1 when every line's factor couples
   // neighbouring elements through face nodes only (launch_band_lines_structure)
   int lines_sparse;
-  // the same factors rearranged per element block for the warp-per-line solve
-  // (launch_linewarp_prep), or null
-  const double* lines_blocks;
 };
 void launch_band_solve(const BandSolve& B, cudaStream_t st);
 // number of entries of the per-line factors (ld = nlines) outside the
 // face-node coupling structure that are not zero, added to *count
 void launch_band_lines_structure(const LineMap& M, const double* band, int* count, cudaStream_t st);
-// doubles of the per-element-block rearrangement of per-line factors for the
-// warp-per-line solve (0 when the block is wider than a warp or ns is not 4 / 5)
-size_t linewarp_doubles(const LineMap& M);
-void launch_linewarp_prep(const LineMap& M, const double* band, double* blocks, cudaStream_t st);
 void launch_block_prep(const double* band, int KV, int BW1, double* blk, cudaStream_t st);
 // the per-element tiles of the warp-owned solve (band_solve_warp_kernel)
 size_t frag_doubles(int KV, int BW1, int NS);

@@ -429,3 +429,4 @@ def test_sphere_fused_stage_equals_two_launches(orc, vflux):
     bound = np.maximum(1e-12, PT.SPREAD_FACTOR * PT.field_rel_errors(o2, o))
     print(f"[parity] sphere fused vs two launches ({vflux}): {err}, bound {bound}")
     assert np.all(err <= bound), (err, bound)
+
