@@ -138,14 +138,34 @@ __device__ __forceinline__ void pair_contract(const LawP& L, const double* q1, c
       const double b1 = P1[4], b2 = P2[4];
       const double b_avg = (b1 + b2) / 2.0;
       const double u2_avg = (P1[5] + P2[5]) / 2.0;
-      rho_m = logavg_fast(r1, r2);
-      const double b_log = logavg_fast(b1, b2);
-      const double rinv = 1.0 / (b_avg * b_log);
-      pc = rho_avg * b_log * rinv / 2.0;
-      double c1 = b_avg * rinv / (2.0 * (L.gamma - 1.0)) - u2_avg / 2.0;
+      // with both logarithmic means on their series branch (the common case
+      // within an element) every division shares one reciprocal,
+      // 1 / ((r1+r2)^2 (b1+b2)^2): rho_log = rho_avg G(u_rho),
+      // rho_avg / (2 b_avg) = rho_avg / (b1+b2), 1 / (2 (gamma-1) b_log) =
+      // F(u_b) / ((gamma-1) (b1+b2)) -- as the brick kernels' ec_vol
+      const double rs = r1 + r2, rd = r1 - r2, bs = b1 + b2, bd = b1 - b2;
+      const double rs2 = rs * rs, bs2 = bs * bs, rd2 = rd * rd, bd2 = bd * bd;
+      double cterm;
+      if (rd2 < 1e-2 * rs2 && bd2 < 1e-2 * bs2) {
+        const double inv = 1.0 / (rs2 * bs2);
+        const double ur = rd2 * bs2 * inv, ub = bd2 * rs2 * inv;
+        const double inv_bs = bs * rs2 * inv;
+        rho_m = rho_avg * series_G(ur);
+        pc = rho_avg * inv_bs;
+        cterm = series_F(ub) * inv_bs / (L.gamma - 1.0);
+      } else {
+        rho_m = logavg_fast(r1, r2);
+        const double b_log = logavg_fast(b1, b2);
+        const double rinv = 1.0 / (b_avg * b_log);
+        pc = rho_avg * b_log * rinv / 2.0;
+        cterm = b_avg * rinv / (2.0 * (L.gamma - 1.0));
+      }
+      double c1 = cterm - u2_avg / 2.0;
       if (LAW == LAW_EG) {
         c1 = c1 + (Phi1 + Phi2) / 2.0;
-        fl = (b_avg * rho_m / (2.0 * b1)) * (Phi1 - Phi2);
+        // alpha = b_avg rho_log / (2 b1), with 1 / (2 b1) = p1 / rho1 from the
+        // node's point values
+        fl = (b_avg * rho_m * P1[7]) * (Phi1 - Phi2);
       }
       c4 = c1 + dot<3>(ua, ua);
     } else {
