@@ -67,6 +67,7 @@ SIGNATURES = {
     "atb_op_instances": [_VP, _IP, _IP],
     "atb_op_autotune": [_VP, PtrArr, _DP, _VP, _IP],
     "atb_op_set_launch": [_VP, C.c_int],
+    "atb_op_set_persistent": [_VP, C.c_int],
     "atb_op_set_active": [_VP, C.c_int],
     "atb_op_create_pool": [C.POINTER(OpDesc), C.c_int, C.POINTER(C.c_void_p)],
     "atb_op_place_instance": [_VP, C.c_int, C.POINTER(OpDesc), _DP, _VP],

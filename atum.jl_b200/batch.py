@@ -25,7 +25,7 @@ import numpy as np
 from . import _lib
 from ._device import make_desc
 
-__all__ = ["PackedDGSEM", "set_instance_dt", "autotune", "set_launch"]
+__all__ = ["PackedDGSEM", "set_instance_dt", "autotune", "set_launch", "set_persistent"]
 
 
 class _PackedDevice:
@@ -104,6 +104,9 @@ class PackedDGSEM:
     def set_launch(self, elements_per_cta: int):
         set_launch(self, elements_per_cta)
 
+    def set_persistent(self, ctas: int):
+        set_persistent(self, ctas)
+
 
 def autotune(dg, q) -> int:
     """Pick the elements-per-CTA launch shape of a ``DGSEM`` or ``PackedDGSEM``
@@ -122,6 +125,13 @@ def autotune(dg, q) -> int:
 
 def set_launch(dg, elements_per_cta: int):
     _lib.check(_lib.lib().atb_op_set_launch(dg.device.h, int(elements_per_cta)))
+
+
+def set_persistent(dg, ctas: int):
+    """Persistent tendency launches of at most ``ctas`` CTAs that walk the
+    element tiles of every packed instance with a grid stride (0: one CTA per
+    tile).  Results do not depend on it."""
+    _lib.check(_lib.lib().atb_op_set_persistent(dg.device.h, int(ctas)))
 
 
 def set_instance_dt(solver, dts):

@@ -171,6 +171,8 @@ struct atb_op {
   int prof_class = ATB_PROF_TEND;
   int E = 1;
   size_t smem = 0;
+  int persist_ctas = 0;  // > 0: persistent launches of at most this many CTAs (brick kernels)
+  tend_launch_fn launch_persist = nullptr;  // the persistent variant of `launch`
   // curved elements (atb_op_create_curved): per-node metrics and M J, per
   // face node normals, face masses and neighbour nodes, the D matrix
   bool curved = false;
@@ -262,9 +264,14 @@ int run_tendency(atb_op* op, int epi, const double* const* q, double* const* out
   const size_t smem = op->smem;  // plain kernels: no epilogue prefetch (A.pf = 0)
   int grid = (op->K_active + op->E - 1) / op->E;
   if (grid == 0) return ATB_OK;
+  tend_launch_fn fn = op->launch;
+  if (op->persist_ctas > 0) {
+    fn = op->launch_persist;
+    if (grid > op->persist_ctas) grid = op->persist_ctas;
+  }
   {
     ProfScope ps(op->prof_class, st);
-    op->launch(A, grid, cta_threads(op->E, op->Np), smem, st);
+    fn(A, grid, cta_threads(op->E, op->Np), smem, st);
   }
   return check_launch("tendency");
 }
@@ -902,6 +909,20 @@ extern "C" int atb_op_autotune(atb_op* op, const double* const* q, double* scrat
   return check_launch("autotune");
 }
 
+extern "C" int atb_op_set_persistent(atb_op* op, int ctas) {
+  if (!op || ctas < 0) return fail(ATB_ERR_INVALID, "bad argument");
+  if (ctas > 0) {
+    tend_launch_fn fn = op->curved ? nullptr
+                                   : pick_launcher_persistent(op->law.kind, op->dim, op->vk, op->Nq, op->sflux, false, 0);
+    if (!fn)
+      return fail(ATB_ERR_INVALID, "no persistent kernel for this operator (brick, Rusanov surface flux, N = 3..5: "
+                                   "3-D Euler-gravity EC, 2-D Euler EC, 2-D shallow water EC / FP32-flux EC)");
+    op->launch_persist = fn;
+  }
+  op->persist_ctas = ctas;
+  return ATB_OK;
+}
+
 extern "C" int atb_op_set_launch(atb_op* op, int elements_per_cta) {
   if (!op || elements_per_cta < 1 || cta_threads(elements_per_cta, op->Np) > 512 ||
       op_smem(op, elements_per_cta) > 227 * 1024)
@@ -1464,11 +1485,20 @@ int run_fused(atb_solver* s, double* const* Q, const ArkAcc& ark, cudaStream_t s
     A.out[c] = Q[c];  // not read by the fused epilogue
     A.out2[c] = nullptr;
   }
-  const int grid = (op->K_active + E - 1) / E;
+  int grid = (op->K_active + E - 1) / E;
   if (grid == 0) return ATB_OK;
+  tend_launch_fn fn = s->fused;
+  if (op->persist_ctas > 0) {
+    // the persistent fused stage kernel, where one is compiled
+    if (tend_launch_fn fp = pick_launcher_persistent(op->law.kind, op->dim, op->vk, op->Nq, op->sflux, true,
+                                                     s->lin->sflux)) {
+      fn = fp;
+      if (grid > op->persist_ctas) grid = op->persist_ctas;
+    }
+  }
   {
     ProfScope ps(ATB_PROF_TEND, st);
-    s->fused(A, grid, cta_threads(E, op->Np), bytes(E), st);
+    fn(A, grid, cta_threads(E, op->Np), bytes(E), st);
   }
   const cudaError_t le = cudaGetLastError();
   if (le != cudaSuccess)

@@ -313,7 +313,12 @@ __host__ __device__ constexpr int fused_min_blocks(int nq, bool cmp = false) {
 // SF >= 0: the surface flux kind (of the explicit operator and, fused, of the
 // linear one) is a compile-time constant, so the kernel carries one numerical
 // flux instead of all of them; SF = -1 reads it from the arguments.
-template <int LAW, int DIM, int VK, int NQ_, bool FUSE = false, int SF = -1>
+//
+// PERSIST: a persistent launch -- fewer CTAs than tiles of E elements, each
+// CTA walking the tiles (of every packed instance) with a grid stride and
+// restaging shared memory for each; otherwise one CTA per tile.  The tile's
+// work is the same code either way (tile_body).
+template <int LAW, int DIM, int VK, int NQ_, bool FUSE = false, int SF = -1, bool PERSIST = false>
 __global__ void __launch_bounds__(
     FUSE ? fused_max_threads(NQ_, LAW == LAW_EG && fused_compact_fits(NQ_, DIM, NSt<LAW, DIM>::v, NPre<LAW, DIM, VK>::v,
                                                                         NPairVals<LAW, DIM, VK>::stride))
@@ -345,8 +350,6 @@ __global__ void __launch_bounds__(
   constexpr bool CMP = FUSE && LAW == LAW_EG && fused_compact_fits(NQ_, DIM, NS, NPRE, NPVS);
   const int slot = threadIdx.x / Np;
   const int node = threadIdx.x - slot * Np;
-  const int e = blockIdx.x * A.E + slot;
-  const bool act = (slot < A.E) && (e < A.K);
   const int tabn = 2 * Nq * Nq + 2;
   double* sC = sm;            // Cfd
   double* sW = sm + Nq * Nq;  // Cw
@@ -375,6 +378,9 @@ __global__ void __launch_bounds__(
     spair[threadIdx.x] = a | ((a + 1 + p) << 8);
   }
   const LawP& L = A.law;
+  auto tile_body = [&](const int tile) {
+  const int e = tile * A.E + slot;
+  const bool act = (slot < A.E) && (e < A.K);
   const size_t gid = (size_t)e * Np + node;
   // Fused ARK stages: the epilogue's own-node inputs (the accumulators) are
   // copied into shared memory now, asynchronously, so their latency hides
@@ -698,7 +704,7 @@ __global__ void __launch_bounds__(
     for (int v = threadIdx.x; v < A.E * per_elem; v += blockDim.x) {
       const int es = v / per_elem, r = v - es * per_elem;
       const int dd = r / fp, tt = r - dd * fp;
-      const int ef = blockIdx.x * A.E + es;
+      const int ef = tile * A.E + es;
       if (tt >= 2 * Nfp || ef >= A.K) continue;
       double* const sqe = sm + tabn + es * slotsz;
       double* const sae = sqe + NS * Np;
@@ -843,22 +849,38 @@ __global__ void __launch_bounds__(
       }
       break;
   }
+  };  // tile_body
+  if constexpr (PERSIST) {
+    const int ntiles = (A.K + A.E - 1) / A.E;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+      tile_body(tile);
+      __syncthreads();  // the next tile restages shared memory
+    }
+  } else {
+    tile_body(blockIdx.x);
+  }
 }
 
 // launcher signature used by the host dispatch table
 typedef void (*tend_launch_fn)(const TendArgs& A, int grid, int block, size_t smem, cudaStream_t st);
 
-template <int LAW, int DIM, int VK, int NQ_ = 0, bool FUSE = false, int SF = -1>
+template <int LAW, int DIM, int VK, int NQ_ = 0, bool FUSE = false, int SF = -1, bool PERSIST = false>
 void tend_launch(const TendArgs& A, int grid, int block, size_t smem, cudaStream_t st) {
   static size_t configured = 0;
   if (smem > 48 * 1024 && smem > configured) {
     // on failure the launch below reports the error
-    if (cudaFuncSetAttribute(tendency_kernel<LAW, DIM, VK, NQ_, FUSE, SF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) == cudaSuccess)
+    if (cudaFuncSetAttribute(tendency_kernel<LAW, DIM, VK, NQ_, FUSE, SF, PERSIST>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess)
       configured = smem;
   }
-  tendency_kernel<LAW, DIM, VK, NQ_, FUSE, SF><<<grid, block, smem, st>>>(A);
+  tendency_kernel<LAW, DIM, VK, NQ_, FUSE, SF, PERSIST><<<grid, block, smem, st>>>(A);
 }
+
+// persistent variants (atb_op_set_persistent) of the hot configurations: the
+// explicit Rusanov kernels of 3-D Euler-gravity, 2-D Euler and 2-D shallow
+// water (FP64 and FP32 flux) and the fused Euler-gravity ARK23 stage, for
+// the orders N = 3..5; nullptr when there is none
+tend_launch_fn pick_launcher_persistent(int law, int dim, int vk, int nq, int sflux, bool fused, int lin_sflux);
 
 // Euler-gravity explicit tendency fused with the weak-form linear operator
 // along z (ARK23 stages, split_rhs = false): 3-D, EC / FP32-flux EC volume

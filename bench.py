@@ -1077,6 +1077,17 @@ def run_swbatch(args):
     with ClockSampler(torch.cuda.current_device()) as clk:
         ms32 = timed(p32, q32, steps, args.warmup)
     ms64 = timed(p64, q64, steps, args.warmup)
+    # persistent launches of the packed FP32-flux operator: k CTAs per SM walk
+    # every instance's element tiles with a grid stride (same results)
+    nsm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    persist = {}
+    for k in (2, 4, 8, 16):
+        qp = q0.clone()
+        p32.set_persistent(nsm * k)
+        msp = max_over_ranks(timed(p32, qp, steps, args.warmup), dist)
+        persist[f"{k}_per_sm"] = {"ctas": nsm * k, "value": world * dofs * 5 * steps / (msp * 1e-3),
+                                  "ms_per_step": msp / steps, "bitwise_equal_to_ordinary": bool(torch.equal(qp, q32))}
+    p32.set_persistent(0)
     # plain FP64 path: the same instances one at a time (sample of 8)
     nseq = min(8, n_inst)
     qs = [torch.as_tensor(c.q0, device="cuda").contiguous() for c in c64[:nseq]]
@@ -1134,6 +1145,7 @@ def run_swbatch(args):
                    "l2": f"working set ~{3 * dofs * 8 / 1e9:.2f} GB > 126 MB L2 (no flush)",
                    "elements_per_cta": {"fp32flux": E32, "fp64": E64}},
         "packed_fp64": {"value": v64, "ms_per_step": ms64 / steps},
+        "packed_fp32flux_persistent": persist,
         "plain_fp64_one_instance_at_a_time": {"value": vseq, "ms_per_step_per_instance": ms_seq / steps / nseq,
                                                "sample_instances": nseq},
         "speedup_vs_plain_fp64": v32 / vseq,

@@ -206,6 +206,15 @@ int atb_op_copy_instance_aux(atb_op* op, int dst, int src, void* stream);
  * it.  Results do not depend on the shape.  atb_op_set_launch sets it. */
 int atb_op_autotune(atb_op* op, const double* const* q, double* scratch, void* stream, int* chosen);
 int atb_op_set_launch(atb_op* op, int elements_per_cta);
+/* Persistent launches (no reference counterpart): with ctas > 0 every tendency
+ * launch of the operator (its fused ARK23 stages included) runs at most `ctas`
+ * CTAs, each walking the element tiles -- across all packed instances,
+ * whatever their sizes -- with a grid stride; 0 restores one CTA per tile.
+ * Results do not depend on it.  Persistent kernels exist for brick operators
+ * with the Rusanov surface flux at N = 3..5: 3-D Euler-gravity (EC volume
+ * flux; with ARK23 also the fused stage), 2-D Euler (EC), 2-D shallow water
+ * (EC, FP32-flux EC); ATB_ERR_INVALID otherwise. */
+int atb_op_set_persistent(atb_op* op, int ctas);
 
 /* (dg::DGSEM)(dq, q, time; increment) -- src/dgsem.jl:59-98 */
 int atb_op_apply(atb_op* op, double* const* dq, const double* const* q, double time, int increment, void* stream);
