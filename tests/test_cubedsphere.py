@@ -226,6 +226,19 @@ def test_oracle_curved_path_on_brick_geometry(orc, weak):
         assert np.array_equal(d1, d2), PT.field_rel_errors(d2, d1)
 
 
+def test_sphere_vtu_snapshot(tmp_path):
+    """VTK snapshots of sphere fields (the experiments' output): the nodes of
+    every curved element as points, N^3 linear sub-cells per element."""
+    import xml.etree.ElementTree as ET
+    from atum_b200 import vtk
+    case = W.sphere_acoustic_wave(N=2, KH=1, KV=2)
+    g = case.dg.grid
+    path = vtk.write_vtu(str(tmp_path / "sphere.vtu"), g, {"rho": case.q0[0]})
+    piece = ET.parse(path).getroot().find(".//Piece")
+    assert int(piece.get("NumberOfPoints")) == g.K * g.cell.Np
+    assert int(piece.get("NumberOfCells")) == g.K * (g.cell.Nq - 1) ** 3
+
+
 def test_curved_abi_checks_without_gpu():
     from atum_b200 import _lib
     from atum_b200._device import make_desc
