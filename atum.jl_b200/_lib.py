@@ -43,6 +43,8 @@ PtrArr = C.c_void_p * 5
 _LIB = None
 # int (*)(double ex_time, double im_time, double* const* q_stage, void* user)
 STAGE_CB = C.CFUNCTYPE(C.c_int, C.c_double, C.c_double, C.POINTER(C.c_void_p), C.c_void_p)
+# int (*)(double* const* state, void* user): atb_solver_set_exchange_callback
+EXCHANGE_CB = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_void_p), C.c_void_p)
 
 # exported entry points and their argtypes (every one returns int status)
 _VP, _DP, _IP = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int)
@@ -97,6 +99,7 @@ SIGNATURES = {
     "atb_launch_count": [C.POINTER(C.c_long)],
     "atb_lsrk54_step_noalloc": [_VP, PtrArr, C.c_double, C.c_int, _VP],
     "atb_solver_set_stage_callback": [_VP, STAGE_CB, _VP],
+    "atb_solver_set_exchange_callback": [_VP, EXCHANGE_CB, _VP],
 }
 
 

@@ -1057,6 +1057,8 @@ struct atb_solver {
   // after_stage (src/odesolvers.jl:10-11,23): host callback between stages
   atb_stage_callback stage_cb = nullptr;
   void* stage_user = nullptr;
+  atb_exchange_callback xchg_cb = nullptr;  // before every tendency of a new state
+  void* xchg_user = nullptr;
 };
 
 namespace {
@@ -1251,6 +1253,17 @@ int call_stage(atb_solver* s, double ex_time, double im_time, double* const* qs)
   return ATB_OK;
 }
 
+// the exchange hook: the state every tendency of the next launch reads,
+// before that launch is enqueued (a sharded run fills its ghost elements)
+int call_exchange(atb_solver* s, double* const* qs) {
+  if (!s->xchg_cb) return ATB_OK;
+  double* p[5];
+  for (int c = 0; c < 5; ++c) p[c] = qs[c < s->ns ? c : 0];
+  const int r = s->xchg_cb(p, s->xchg_user);
+  if (r != 0) return fail(ATB_ERR_CALLBACK, "exchange callback returned %d", r);
+  return ATB_OK;
+}
+
 // LSRK stages with a stage callback: the stage kernel writes the new state to
 // qB and it is copied back into q before the callback, so the callback always
 // sees (and may change) the caller's q, and the next stage starts from it.
@@ -1263,8 +1276,10 @@ int lsrk_steps_cb(atb_solver* s, double* const* q, int nsteps, cudaStream_t st) 
   for (int k = 0; k < 5; ++k) cur[k] = q[k < s->ns ? k : 0];
   for (int n = 0; n < nsteps; ++n) {
     for (size_t i = 0; i < s->rka.size(); ++i) {
-      int rc = s->d_dte ? run_tendency(op, EPI_LSRK, cur, dq, qb, s->rka[i], s->rkb[i], st, s->d_dte)
-                        : run_tendency(op, EPI_LSRK, cur, dq, qb, s->rka[i], s->rkb[i] * s->dt, st);
+      int rc = call_exchange(s, cur);
+      if (rc) return rc;
+      rc = s->d_dte ? run_tendency(op, EPI_LSRK, cur, dq, qb, s->rka[i], s->rkb[i], st, s->d_dte)
+                    : run_tendency(op, EPI_LSRK, cur, dq, qb, s->rka[i], s->rkb[i] * s->dt, st);
       if (rc) return rc;
       if ((rc = copy_field(q, qb, s->ns, (size_t)op->K_active * op->Np, st))) return rc;
       const double t = s->time + s->rkc[i] * s->dt;
@@ -1285,8 +1300,10 @@ int lsrk_steps(atb_solver* s, double* const* q, int nsteps, cudaStream_t st) {
   bool in_user = true;
   for (int n = 0; n < nsteps; ++n) {
     for (size_t st_ = 0; st_ < s->rka.size(); ++st_) {
-      int rc = s->d_dte ? run_tendency(op, EPI_LSRK, cur, dq, oth, s->rka[st_], s->rkb[st_], st, s->d_dte)
-                        : run_tendency(op, EPI_LSRK, cur, dq, oth, s->rka[st_], s->rkb[st_] * s->dt, st);
+      int rc = call_exchange(s, cur);
+      if (rc) return rc;
+      rc = s->d_dte ? run_tendency(op, EPI_LSRK, cur, dq, oth, s->rka[st_], s->rkb[st_], st, s->d_dte)
+                    : run_tendency(op, EPI_LSRK, cur, dq, oth, s->rka[st_], s->rkb[st_] * s->dt, st);
       if (rc) return rc;
       for (int k = 0; k < 5; ++k) std::swap(cur[k], oth[k]);
       in_user = !in_user;
@@ -1310,6 +1327,7 @@ int rlsrk_step(atb_solver* s, double* const* q, cudaStream_t st) {
   double eta0 = 0, deta = -0.0;
   if ((rc = atb_entropyintegral(op, q0, &eta0, st))) return rc;
   for (size_t i = 0; i < s->rka.size(); ++i) {
+    if ((rc = call_exchange(s, q))) return rc;
     if ((rc = run_tendency(op, EPI_RLSRK, q, k, dq, s->rka[i], 0, st))) return rc;
     double ep = 0;
     if ((rc = atb_entropyproduct(op, q, k, &ep, st))) return rc;
@@ -1552,8 +1570,9 @@ int ark_step_accumulated(atb_solver* s, double* const* q, cudaStream_t st) {
   ArkAcc a;
   // one stage: N(Q) then L(Q) with the accumulation, or both in one launch
   auto stage = [&](double* const* Q) -> int {
-    if (s->fuse_on) return run_fused(s, Q, a, st);
     int r;
+    if ((r = call_exchange(s, Q))) return r;
+    if (s->fuse_on) return run_fused(s, Q, a, st);
     if ((r = run_tendency(s->rhs, EPI_SET, Q, N, nullptr, 0, 0, st))) return r;
     return run_tendency(s->lin, EPI_ARK, Q, N, nullptr, 0, 0, st, nullptr, &a);
   };
@@ -1602,6 +1621,7 @@ int ark_step(atb_solver* s, double* const* q, cudaStream_t st) {
   }
   auto eval = [&](int i) -> int {
     int rc;
+    if ((rc = call_exchange(s, Q[i]))) return rc;
     if (s->rhs) {
       if ((rc = run_tendency(s->rhs, EPI_SET, Q[i], ex[i], nullptr, 0, 0, st))) return rc;
     } else {
@@ -1913,6 +1933,13 @@ extern "C" int atb_solver_set_instance_dt(atb_solver* s, const double* dt_host) 
   if (!s->d_dte && (rc = dalloc(&s->d_dte, (size_t)op->K))) return rc;
   s->own_dte = true;
   CK(cudaMemcpy(s->d_dte, dte.data(), dte.size() * sizeof(double), cudaMemcpyHostToDevice));
+  return ATB_OK;
+}
+
+extern "C" int atb_solver_set_exchange_callback(atb_solver* s, atb_exchange_callback cb, void* user) {
+  if (!s) return fail(ATB_ERR_INVALID, "null solver");
+  s->xchg_cb = cb;
+  s->xchg_user = cb ? user : nullptr;
   return ATB_OK;
 }
 

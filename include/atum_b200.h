@@ -279,6 +279,16 @@ int atb_solver_set_element_dt(atb_solver* s, const double* dte_device);
  * the reference passes a Julia closure.) */
 typedef int (*atb_stage_callback)(double ex_time, double im_time, double* const* q_stage, void* user);
 int atb_solver_set_stage_callback(atb_solver* s, atb_stage_callback cb, void* user);
+/* Exchange hook (no reference counterpart; the element-slab sharding of one
+ * problem over several GPUs, atum_b200.sharded): cb(state, user) runs on the
+ * host before every tendency launch that reads a new state -- each LSRK /
+ * RLSRK stage (the stage's input state) and each ARK23 stage (q, then the
+ * stage states Q_2, Q_3 after their solves) -- with the Ns device pointers of
+ * that state; it fills the state's ghost elements with work ordered on the
+ * solver's stream.  A nonzero return stops the step with ATB_ERR_CALLBACK.
+ * NULL clears it.  Not called by atb_lsrk54_step_noalloc. */
+typedef int (*atb_exchange_callback)(double* const* state, void* user);
+int atb_solver_set_exchange_callback(atb_solver* s, atb_exchange_callback cb, void* user);
 
 /* measures -- src/measures.jl:6-33 (p = 2 or INFINITY); results to host memory */
 int atb_weightednorm(atb_op* op, const double* const* q, double p, double* comp_host, double* total_host,

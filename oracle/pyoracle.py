@@ -209,6 +209,23 @@ class Solver:
         self._cb = _STAGE_CB(cb)
         lib().orc_set_stage_callback(self.h, self._cb, None)
 
+    def set_stage_hook(self, fn):
+        """``fn(q)`` after every stage with the solver's own state as a
+        writable array (no copy): what it writes is what the next stage reads
+        (a sharded run's ghost exchange).  None clears it."""
+        if fn is None:
+            self._cb = None
+            lib().orc_set_stage_callback(self.h, _STAGE_CB(), None)
+            return
+        any_ = self.rhs if self.rhs is not None else self.linrhs
+        shape = (any_.ns, any_.K, any_.Np)
+
+        def cb(ex_t, im_t, qp, user):
+            fn(np.ctypeslib.as_array(qp, shape=shape))
+
+        self._cb = _STAGE_CB(cb)
+        lib().orc_set_stage_callback(self.h, self._cb, None)
+
 
 def LSRK54(dg, q, dt, t0=0.0):
     return Solver("LSRK54", dg, dt, t0)
