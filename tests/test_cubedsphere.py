@@ -289,8 +289,8 @@ def _tendency_cases():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", list(_tendency_cases()))
-@pytest.mark.parametrize("N", [2, 3, 5])
+@pytest.mark.parametrize("name,N", [(n, N) for N in (2, 3, 5) for n in _tendency_cases()] +
+                         [(n, N) for N in (1, 7) for n in ("eg-ec-rusanov", "eg-weak-rusanov", "leg-weak-z")])
 def test_curved_tendency_matches_oracle(orc, name, N):
     """Seeded states 5% away from the zonal flow's balanced reference state;
     plain field-relative error per component against max(1e-12, 10 x the
