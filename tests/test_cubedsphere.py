@@ -265,6 +265,13 @@ def test_curved_abi_checks_without_gpu():
 
 
 # --------------------------------------------------------------------- GPU
+def _rotating(dg):
+    law = dg.law
+    pr = A.Coriolis((0.0, 0.0, 2 * 7.29212e-5 * 125), bc=law.problem.bc, referencestate=law.problem.referencestate)
+    rot = A.EulerGravityLaw(3, sphere=True, grav=law.grav, problem=pr)
+    return A.DGSEM(law=rot, grid=dg.grid, volume_form=dg.volume_form, surface_numericalflux=dg.surface_numericalflux)
+
+
 def _tendency_cases():
     zon = lambda: W.sphere_zonal_flow(N=3, KH=2, KV=2)  # noqa: E731
     return {
@@ -284,6 +291,9 @@ def _tendency_cases():
                                          volume_form=A.FluxDifferencingForm(A.EntropyConservativeFlux()),
                                          surface_numericalflux=A.MatrixFlux()), None),
         "leg-weak-z": lambda: (zon().lindg, None),
+        # the baroclinic wave's rotating sphere: dq[rho u] -= (0, 0, 2 Omega) x rho u
+        # (experiment/euler_gravity/baroclinicwave.jl:27-34)
+        "eg-ec-rusanov-coriolis": lambda: (_rotating(zon().dg), None),
         "euler-ec-kg": lambda: (None, "euler"),
     }
 
