@@ -15,6 +15,9 @@ library and the CPU oracle.
   shell (experiment/euler_gravity/acousticwave.jl), N=5, KH=10, KV=5, IMEX ARK23
 * ``sphere_zonal_flow``     isothermal zonal flow on a small-planet shell
   (experiment/euler_gravity/isothermal_zonal_flow.jl), N=3, KH=KV=5, IMEX ARK23
+* ``sphere_baroclinic_wave``  deep-atmosphere baroclinic wave on a rotating
+  Earth-radius shell (experiment/euler_gravity/baroclinicwave.jl), N=3, KH=8,
+  KV=4, IMEX ARK23
 """
 from __future__ import annotations
 
@@ -254,6 +257,75 @@ def sphere_zonal_flow(N=3, KH=5, KV=5, steps=10, imex=True, dt=None, vflux="ec")
 
     dt = dt if dt is not None else 3 * min_node_distance(grid, dims=(3,)) / 330.0
     return _sphere_case("sphere_zonal_flow", law, grid, q0, dt, steps, imex, vflux)
+
+
+def sphere_baroclinic_wave(N=3, KH=8, KV=4, steps=10, imex=True, dt=None, vflux="ec", perturb=True):
+    """Baroclinic wave on a rotating Earth-radius shell 30 km deep
+    (baroclinicwave.jl:49-253): the deep-atmosphere balanced state of
+    Ullrich, Melvin, Jablonowski and Staniforth (2014) with T_E = 310 K,
+    T_P = 240 K, lapse rate 0.005 K/m, k = 3, b = 2, and a zonal-wind
+    perturbation of 1 m/s centred at (20 deg E, 40 deg N); g = 9.80616,
+    Omega = 7.29212e-5 (the Coriolis source dq[rho u] -= (0, 0, 2 Omega) x rho u),
+    reflective inner and outer spheres, isothermal (300 K) reference state;
+    EC volume flux, Rusanov surface flux, IMEX ARK23 (split_rhs = false) with
+    dt = 3 dz / 330."""
+    a, top, Om, grav = _EARTH_RADIUS, 30e3, 7.29212e-5, 9.80616
+    problem = Coriolis((0.0, 0.0, 2 * Om), bc=ReflectiveWall().bc, referencestate=_isothermal_reference(a))
+    law = EulerGravityLaw(3, sphere=True, grav=grav, problem=problem)
+    cell = LobattoCell(N + 1, N + 1, N + 1)
+    grid = cubedspheregrid(cell, _vec(a, a + top, KV), KH)
+
+    def q0(dg):
+        x = grid.points()
+        Phi = dg.auxstate_host()[0]
+        cv_d = 719.0
+        R_d = law.gamma * cv_d - cv_d
+        r = np.sqrt(np.sum(x * x, axis=0))
+        z = r - a
+        lon = np.arctan2(x[1], x[0])
+        lat = np.arcsin(x[2] / r)
+        k, T_E, T_P, Gam, b, p_0 = 3.0, 310.0, 240.0, 0.005, 2.0, 1e5
+        T_0 = (T_E + T_P) / 2
+        A_, B_ = 1 / Gam, (T_0 - T_P) / T_0 / T_P
+        C_ = (k + 2) / 2 * (T_E - T_P) / T_E / T_P
+        H = R_d * T_0 / grav
+        z_t, lon_c, lat_c, d_0, V_p = 15e3, np.pi / 9, 2 * np.pi / 9, a / 6, 1.0
+        tz1 = np.exp(Gam * z / T_0)
+        tz2 = 1 - 2 * (z / b / H) ** 2
+        tz3 = np.exp(-(z / b / H) ** 2)
+        tau1 = 1 / T_0 * tz1 + B_ * tz2 * tz3
+        tau2 = C_ * tz2 * tz3
+        ti1 = A_ * (tz1 - 1) + B_ * z * tz3
+        ti2 = C_ * z * tz3
+        cz = np.cos(lat) * (1 + z / a)  # deep atmosphere
+        I_T = cz ** k - k / (k + 2) * cz ** (k + 2)
+        T = 1 / (tau1 - tau2 * I_T)
+        p = p_0 * np.exp(-grav / R_d * (ti1 - ti2 * I_T))
+        U = grav * k / a * ti2 * T * (cz ** (k - 1) - cz ** (k + 1))
+        rc = (a + z) * np.cos(lat)
+        u = -Om * rc + np.sqrt((Om * rc) ** 2 + rc * U)
+        v = np.zeros_like(u)
+        if perturb:
+            F_z = np.where(z > z_t, 0.0, 1 - 3 * (z / z_t) ** 2 + 2 * (z / z_t) ** 3)
+            cosd = np.sin(lat) * np.sin(lat_c) + np.cos(lat) * np.cos(lat_c) * np.cos(lon - lon_c)
+            d = a * np.arccos(np.clip(cosd, -1.0, 1.0))
+            inside = (d > 0) & (d < d_0)
+            c3 = np.cos(np.pi * d / 2 / d_0) ** 3
+            s1 = np.sin(np.pi * d / 2 / d_0)
+            sd = np.where(inside, np.sin(d / a), 1.0)
+            amp = np.where(inside, 16 * V_p / 3 / np.sqrt(3) * F_z * c3 * s1 / sd, 0.0)
+            u = u + amp * -(-np.sin(lat_c) * np.cos(lat) + np.cos(lat_c) * np.sin(lat) * np.cos(lon - lon_c))
+            v = v + amp * np.cos(lat_c) * np.sin(lon - lon_c)
+        # spherical (east, north, up) to Cartesian components
+        uc = -np.sin(lon) * u - np.sin(lat) * np.cos(lon) * v
+        vc = np.cos(lon) * u - np.sin(lat) * np.sin(lon) * v
+        wc = np.cos(lat) * v
+        rho = p / (R_d * T)
+        ke = (uc ** 2 + vc ** 2 + wc ** 2) / 2
+        return _pack(rho, rho * uc, rho * vc, rho * wc, rho * (cv_d * T + ke + Phi))
+
+    dt = dt if dt is not None else 3 * min_node_distance(grid, dims=(3,)) / 330.0
+    return _sphere_case("sphere_baroclinic_wave", law, grid, q0, dt, steps, imex, vflux)
 
 
 # ------------------------------------------------------ shallow water, C3

@@ -385,7 +385,8 @@ def _oracle_steps(orc, case, counts, q0=None, dt=None):
     (lambda: W.sphere_zonal_flow(N=3, KH=2, KV=3, steps=5), (1, 5), (1e-12, 1e-11)),
     (lambda: W.sphere_acoustic_wave(N=3, KH=2, KV=2, steps=3), (1, 3), (1e-12, 1e-11)),
     (lambda: W.sphere_zonal_flow(N=3, KH=2, KV=2, steps=5, imex=False, dt=0.5), (1, 5), (1e-12, 1e-11)),
-], ids=["zonal-ark23", "acoustic-ark23", "zonal-lsrk54"])
+    (lambda: W.sphere_baroclinic_wave(N=3, KH=2, KV=2, steps=3), (1, 3), (1e-12, 1e-11)),
+], ids=["zonal-ark23", "acoustic-ark23", "zonal-lsrk54", "baroclinic-ark23"])
 def test_sphere_steps_match_oracle(orc, build, counts, tol):
     """Bound: max(tol, 10 x the oracle's own rounding spread), the spread being
     the larger change of the oracle's result under a one-ulp move of the
