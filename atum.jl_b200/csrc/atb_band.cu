@@ -26,6 +26,7 @@
 // ev+1 overlaps the arithmetic of element ev, and read back as warp broadcasts.
 #include "atb_generic.cuh"
 
+#include <cstdlib>
 #include <type_traits>
 #include <utility>
 
@@ -829,6 +830,8 @@ __global__ void __launch_bounds__(32 * NW) band_solve_warp_kernel(const BandSolv
   };
   const std::integral_constant<int, 0> fwd{};
   const std::integral_constant<int, 1> bwd{};
+  // the right-hand side may come from the previous kernel of the stream
+  pdl_wait();
   __syncthreads();
   // ------------------------------------------------------------ forward
   // slot: ev % RS; the refill of slot (ev + 2) % RS = (ev - 1) % RS follows
@@ -873,6 +876,7 @@ __global__ void __launch_bounds__(32 * NW) band_solve_warp_kernel(const BandSolv
     }
   }
   cp_async_wait<0>();
+  pdl_trigger();
 }
 
 template <int NQ, int NS, int NW>
@@ -891,7 +895,7 @@ void warp_launch_nw(const BandSolve& B, cudaStream_t st) {
     cudaFuncSetAttribute(band_solve_warp_kernel<NQ, NS, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   configured = true;
   const int warps = (B.M.nlines + 7) / 8;
-  band_solve_warp_kernel<NQ, NS, NW><<<(warps + NW - 1) / NW, 32 * NW, smem, st>>>(B);
+  launch_maybe_pdl(band_solve_warp_kernel<NQ, NS, NW>, dim3((warps + NW - 1) / NW), dim3(32 * NW), smem, st, B);
 }
 
 // Warps per CTA: the element steps are bound by the issue rate of each SM, so
@@ -1153,6 +1157,14 @@ __global__ void band_lines_structure_kernel(const LineMap M, const double* band,
 
 void launch_band_lines_structure(const LineMap& M, const double* band, int* count, cudaStream_t st) {
   band_lines_structure_kernel<<<148 * 8, 256, 0, st>>>(M, band, count);
+}
+
+bool pdl_enabled() {
+  static const int on = [] {
+    const char* e = std::getenv("ATB_PDL");
+    return (e && e[0] == '0') ? 0 : 1;
+  }();
+  return on != 0;
 }
 
 void launch_band_solve(const BandSolve& B, cudaStream_t st) {

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stddef.h>
 
+#include <utility>
+
 namespace atb {
 
 // out = base + dt * sum_k (a_k X_k + b_k Y_k), accumulated in k order like
@@ -88,5 +90,40 @@ bool warp_solve_structure_ok(const double* blk_host, int KV, int BW1, int NS);
 
 void launch_red_finish(const double* partials, int nblocks, int linf, double* out5, cudaStream_t st);
 double probe_fp64_tflops(cudaStream_t st);
+
+// ---------------------------------------------- programmatic dependent launch
+// The stage kernels and the banded solve are launched with programmatic
+// stream serialization: a kernel's grid may start while the previous kernel
+// of its stream drains, runs its prologue (constant tables, pointers, buffer
+// zeroing: nothing the previous kernel writes), and waits in pdl_wait() for
+// the previous grid's completion and memory flush before its first dependent
+// read.  Every such kernel calls pdl_trigger() after its last store, so a
+// dependent grid launches only once all of its CTAs have done their work (a
+// waiting dependent never holds resources one of them needs; triggering at
+// the start, with dependents resident and waiting early, measured slower).  Both instructions are no-ops in
+// a kernel launched without the attribute.  ATB_PDL=0 in the environment
+// launches ordinarily.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+bool pdl_enabled();
+template <typename... KArgs, typename... Args>
+cudaError_t launch_maybe_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                             Args&&... args) {
+  if (!pdl_enabled()) {
+    kern<<<grid, block, smem, st>>>(args...);
+    return cudaSuccess;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
 
 }  // namespace atb

@@ -40,6 +40,7 @@
 //                -- the stage right-hand sides and the final update are
 //                accumulated here, so E and I are never stored
 #pragma once
+#include "atb_generic.cuh"
 #include "atb_physics.cuh"
 
 namespace atb {
@@ -378,6 +379,9 @@ __global__ void __launch_bounds__(
     spair[threadIdx.x] = a | ((a + 1 + p) << 8);
   }
   const LawP& L = A.law;
+  // everything above reads launch constants only; the state, aux and
+  // accumulators below may come from the previous kernel of the stream
+  pdl_wait();
   auto tile_body = [&](const int tile) {
   const int e = tile * A.E + slot;
   const bool act = (slot < A.E) && (e < A.K);
@@ -859,6 +863,7 @@ __global__ void __launch_bounds__(
   } else {
     tile_body(blockIdx.x);
   }
+  pdl_trigger();
 }
 
 // launcher signature used by the host dispatch table
@@ -873,7 +878,7 @@ void tend_launch(const TendArgs& A, int grid, int block, size_t smem, cudaStream
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess)
       configured = smem;
   }
-  tendency_kernel<LAW, DIM, VK, NQ_, FUSE, SF, PERSIST><<<grid, block, smem, st>>>(A);
+  launch_maybe_pdl(tendency_kernel<LAW, DIM, VK, NQ_, FUSE, SF, PERSIST>, dim3(grid), dim3(block), smem, st, A);
 }
 
 // persistent variants (atb_op_set_persistent) of the hot configurations: the
