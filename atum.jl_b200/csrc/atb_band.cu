@@ -1093,6 +1093,9 @@ __global__ void __launch_bounds__(64) band_solve_lines_kernel(const BandSolve B)
   double nb[BW1], cur[BW1];
 #pragma unroll
   for (int j = 0; j < BW1; ++j) nb[j] = cur[j] = 0.0;
+  // the right-hand side may come from the previous kernel of the stream
+  // (programmatic dependent launch, launch_maybe_pdl)
+  pdl_wait();
   // forward: L y = rhs (unit diagonal)
   for (int ev = 0; ev < KV; ++ev) {
     const size_t eoff = (size_t)(e0 + ev * M.estep) * Np + hn;
@@ -1110,11 +1113,12 @@ __global__ void __launch_bounds__(64) band_solve_lines_kernel(const BandSolve B)
 #pragma unroll
     for (int j = 0; j < BW1; ++j) nb[j] = cur[j];
   }
+  pdl_trigger();
 }
 
 typedef void (*lines_fn)(const BandSolve& B, cudaStream_t st);
 template <int NQ, int NS, bool SPARSE> void lines_launch(const BandSolve& B, cudaStream_t st) {
-  band_solve_lines_kernel<NQ, NS, SPARSE><<<(B.M.nlines + 63) / 64, 64, 0, st>>>(B);
+  launch_maybe_pdl(band_solve_lines_kernel<NQ, NS, SPARSE>, dim3((B.M.nlines + 63) / 64), dim3(64), 0, st, B);
 }
 template <int NS, bool SPARSE> lines_fn pick_lines_sp(int nq) {
   switch (nq) {

@@ -414,6 +414,9 @@ __global__ void __launch_bounds__(512) curved_kernel(const TendArgs A) {
   const int e = blockIdx.x * E + el;
   const bool active = el < E && e < A.K;
   for (int i = tid; i < Nq * Nq; i += blockDim.x) sD[i] = A.Dmat[i];
+  // the state, aux and accumulators below may come from the previous kernel
+  // of the stream (programmatic dependent launch, launch_maybe_pdl)
+  pdl_wait();
   double* base = smem + nqq + (size_t)(el < E ? el : 0) * per;
   double* sq = base;
   double* sa = sq + (size_t)NS * Np;
@@ -682,6 +685,7 @@ __global__ void __launch_bounds__(512) curved_kernel(const TendArgs A) {
       }
       break;
   }
+  pdl_trigger();
 }
 
 template <int LAW, int VK, int SF, bool FUSE = false>
@@ -692,7 +696,7 @@ void curved_launch(const TendArgs& A, int grid, int block, size_t smem, cudaStre
                              (int)smem) == cudaSuccess)
       configured = smem;
   }
-  curved_kernel<LAW, VK, SF, FUSE><<<grid, block, smem, st>>>(A);
+  launch_maybe_pdl(curved_kernel<LAW, VK, SF, FUSE>, dim3(grid), dim3(block), smem, st, A);
 }
 
 }  // namespace
